@@ -1,0 +1,192 @@
+// Device helpers shared by the engine's kernels: lane groups, shared-memory
+// hashing, bitonic sorting and block-level scans.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "internal.h"
+
+namespace spg {
+
+// A matrix as the kernels see it (B is A, or the engine's transpose of A).
+struct MatView {
+  int32_t n;
+  int64_t nnz;
+  const int32_t* __restrict__ rowptr;
+  const int32_t* __restrict__ col;
+  const double* __restrict__ val;
+};
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+__device__ __forceinline__ int ld_volatile_shared(const int* p) {
+  return *(const volatile int*)p;
+}
+
+__device__ __forceinline__ void report(uint32_t* status, uint32_t bits) {
+  atomicOr(status, bits);
+}
+
+// Multiply-shift hash: the high bits of j·φ·2^32 select one of 2^LOG2T slots.
+// (The reference keeps the low bits of j·2654435761, src/spgemm_engine.cuh:64,
+// so keys congruent modulo the table size collide; the high bits do not.)
+template <int LOG2T>
+__device__ __forceinline__ unsigned hash_slot(int j) {
+  return ((unsigned)j * 0x9E3779B1u) >> (32 - LOG2T);
+}
+
+// Open-addressing insert with linear probing into a shared table of 2^LOG2T
+// int keys.  A slot is read first (volatile, so every probe sees other lanes'
+// CAS results) and claimed with atomicCAS only when empty.  Returns the slot
+// of `j`, or −1 after 2^LOG2T probes (table full: reported, never spins).
+template <int LOG2T>
+__device__ __forceinline__ int hash_insert(int* keys, int j, uint32_t* status) {
+  constexpr unsigned T = 1u << LOG2T;
+  unsigned h = hash_slot<LOG2T>(j);
+#pragma unroll 1
+  for (unsigned probe = 0; probe < T; ++probe) {
+    int cur = ld_volatile_shared(keys + h);
+    if (cur == j) return (int)h;
+    if (cur == kEmptyKey) {
+      int old = atomicCAS(keys + h, kEmptyKey, j);
+      if (old == kEmptyKey || old == j) return (int)h;
+    }
+    h = (h + 1) & (T - 1);
+  }
+  report(status, DEV_ERR_HASH_FULL);
+  return -1;
+}
+
+// ---- lane groups -------------------------------------------------------------
+// A row is processed by a group of G lanes: a power-of-two slice of one warp
+// (G <= 32, several rows per CTA) or the whole CTA (G = blockDim.x > 32).
+struct WarpGroup {
+  int G;        // lanes in the group (power of two, <= 32)
+  int lane;     // 0..G-1
+  int base;     // first lane of the group within its warp
+  unsigned mask;
+  __device__ __forceinline__ WarpGroup(int g) : G(g) {
+    int wl = threadIdx.x & 31;
+    lane = wl & (g - 1);
+    base = wl & ~(g - 1);
+    mask = (g == 32) ? 0xffffffffu : (((1u << g) - 1u) << base);
+  }
+  __device__ __forceinline__ void sync() const { __syncwarp(mask); }
+  __device__ __forceinline__ unsigned ballot(bool p) const {
+    return (__ballot_sync(mask, p) & mask) >> base;
+  }
+  __device__ __forceinline__ int sum(int v) const {
+    for (int o = G >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o, 32);
+    return v;
+  }
+  __device__ __forceinline__ long long sum64(long long v) const {
+    for (int o = G >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o, 32);
+    return v;
+  }
+};
+
+struct CtaGroup {
+  int G;
+  int lane;
+  __device__ __forceinline__ CtaGroup() : G(blockDim.x), lane(threadIdx.x) {}
+  __device__ __forceinline__ void sync() const { __syncthreads(); }
+};
+
+// Block-wide sum of an int (all threads return the total).  `scratch` holds
+// 32 ints; the call contains two __syncthreads.
+__device__ __forceinline__ long long block_sum64(long long v, long long* scratch) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  int w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) scratch[w] = v;
+  __syncthreads();
+  long long t = 0;
+  for (int i = 0; i < nw; ++i) t += scratch[i];
+  return t;
+}
+
+// Block-wide exclusive scan of an int; returns this thread's prefix and sets
+// *total.  `scratch` holds 33 ints.  Contains two __syncthreads.
+__device__ __forceinline__ int block_exclusive_scan(int v, int* scratch, int* total) {
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  int incl = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  __syncthreads();
+  if (lane == 31) scratch[w] = incl;
+  __syncthreads();
+  int before = 0, all = 0;
+  for (int i = 0; i < nw; ++i) {
+    int s = scratch[i];
+    if (i < w) before += s;
+    all += s;
+  }
+  *total = all;
+  return before + incl - v;
+}
+
+// ---- bitonic sort of (key, value) pairs in shared memory ---------------------
+// Sorts keys[0..P) ascending (P a power of two) carrying vals along, by the G
+// lanes of a group.  Ties cannot occur for the engine's unique keys; padding
+// keys are INT_MAX.
+template <class Grp>
+__device__ __forceinline__ void bitonic_sort_pairs(const Grp& g, int* keys, double* vals, int P) {
+  for (int k = 2; k <= P; k <<= 1) {
+    for (int jj = k >> 1; jj > 0; jj >>= 1) {
+      for (int i = g.lane; i < (P >> 1); i += g.G) {
+        int lo = ((i & ~(jj - 1)) << 1) | (i & (jj - 1));
+        int hi = lo + jj;
+        bool asc = (lo & k) == 0;
+        int klo = keys[lo], khi = keys[hi];
+        if ((klo > khi) == asc) {
+          keys[lo] = khi;
+          keys[hi] = klo;
+          double t = vals[lo];
+          vals[lo] = vals[hi];
+          vals[hi] = t;
+        }
+      }
+      g.sync();
+    }
+  }
+}
+
+template <class Grp>
+__device__ __forceinline__ void bitonic_sort_keys(const Grp& g, int* keys, int P) {
+  for (int k = 2; k <= P; k <<= 1) {
+    for (int jj = k >> 1; jj > 0; jj >>= 1) {
+      for (int i = g.lane; i < (P >> 1); i += g.G) {
+        int lo = ((i & ~(jj - 1)) << 1) | (i & (jj - 1));
+        int hi = lo + jj;
+        bool asc = (lo & k) == 0;
+        int klo = keys[lo], khi = keys[hi];
+        if ((klo > khi) == asc) {
+          keys[lo] = khi;
+          keys[hi] = klo;
+        }
+      }
+      g.sync();
+    }
+  }
+}
+
+__host__ __device__ __forceinline__ int next_pow2_int(int x) {
+  int p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+__host__ __device__ __forceinline__ int ilog2_int(int x) {  // x a power of two
+  int l = 0;
+  while ((1 << l) < x) ++l;
+  return l;
+}
+
+}  // namespace spg

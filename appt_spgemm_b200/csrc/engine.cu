@@ -1,0 +1,873 @@
+// Host orchestration of the engine: context, plan (pre-pass + binning +
+// symbolic), execute (numeric + mirror), multiply, transpose, descriptors and
+// the run_ours-compatible call.
+//
+// The reference's run_ours (src/spgemm_engine.cuh:132-210) allocates and frees
+// every buffer per call, issues at least two blocking 8-byte device→host copies
+// per phase and hands C to nobody.  Here workspace comes from a per-context
+// stream-ordered memory pool, the plan makes three host synchronisations
+// (input validation, bin sizes, nnz(C)), and execute is fully asynchronous and
+// writes C into caller-visible CSR arrays.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+
+namespace spg {
+thread_local long long g_kernel_launches = 0;
+}
+
+using namespace spg;
+
+struct ProfEntry {
+  std::string label;
+  cudaEvent_t a, b;
+};
+
+struct spg_ctx {
+  int device = 0;
+  int num_sms = 148;
+  cudaMemPool_t pool = nullptr;
+  spg_config cfg{};
+  uint32_t* d_status = nullptr;   // device status word (+ scratch, 256 B)
+  int64_t* h_pin = nullptr;       // pinned readback area (512 B)
+  // profiling: per-kernel events on the launching stream, resolved on read
+  bool prof = false;
+  std::vector<ProfEntry> pending;
+  std::map<std::string, std::pair<double, long long>> prof_acc;
+  std::vector<cudaEvent_t> event_pool;
+  long long launch_base = 0;
+};
+
+namespace {
+
+cudaEvent_t prof_event(spg_ctx* c) {
+  if (!c->event_pool.empty()) {
+    cudaEvent_t e = c->event_pool.back();
+    c->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Brackets the kernels launched in its scope with CUDA events when profiling
+// is on; the label names the phase and kernel ("num/bin5", "sym/heavy", ...).
+struct ProfScope {
+  spg_ctx* c;
+  cudaStream_t s;
+  std::string label;
+  cudaEvent_t a = nullptr;
+  ProfScope(spg_ctx* ctx, const char* l, cudaStream_t st, int bin = -1) : c(ctx), s(st) {
+    if (!c->prof) return;
+    label = l;
+    if (bin >= 0) label += std::to_string(bin);
+    a = prof_event(c);
+    cudaEventRecord(a, s);
+  }
+  ~ProfScope() {
+    if (!a) return;
+    cudaEvent_t b = prof_event(c);
+    cudaEventRecord(b, s);
+    c->pending.push_back(ProfEntry{label, a, b});
+  }
+};
+
+void prof_resolve(spg_ctx* c) {
+  for (ProfEntry& e : c->pending) {
+    float ms = 0.f;
+    cudaEventSynchronize(e.b);
+    cudaEventElapsedTime(&ms, e.a, e.b);
+    auto& slot = c->prof_acc[e.label];
+    slot.first += ms;
+    slot.second += 1;
+    c->event_pool.push_back(e.a);
+    c->event_pool.push_back(e.b);
+  }
+  c->pending.clear();
+}
+
+}  // namespace
+
+struct spg_plan {
+  spg_ctx* ctx = nullptr;
+  spg_task task = SPG_TASK_AA;
+  cudaStream_t stream = nullptr;
+  MatView A{}, B{};
+  int32_t n = 0;
+  int G = 8;
+  int64_t* f = nullptr;
+  int32_t* lo = nullptr;
+  int32_t* hi = nullptr;
+  int32_t* rownnz = nullptr;
+  int32_t* rowlow = nullptr;
+  int64_t* rowptr = nullptr;
+  int64_t* lowptr = nullptr;
+  int32_t* rows_num = nullptr;
+  int64_t num_count[kNumBins] = {};
+  int64_t num_start[kNumBins] = {};
+  int64_t nnz_c = 0;
+  int64_t nnz_low = 0;
+  spg_plan_info info{};
+  std::vector<void*> ptrs;
+  int64_t ws_bytes = 0;
+  cudaEvent_t exec_done = nullptr;
+};
+
+namespace {
+
+spg_status cuda_status(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return SPG_OK;
+  cudaGetLastError();  // clear a sticky launch error where possible
+  if (e == cudaErrorMemoryAllocation)
+    return set_error(SPG_ERR_OOM, "%s: %s", what, cudaGetErrorString(e));
+  return set_error(SPG_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define TRY_CUDA(expr, what)                               \
+  do {                                                     \
+    cudaError_t e_ = (expr);                               \
+    if (e_ != cudaSuccess) return cuda_status(e_, (what)); \
+  } while (0)
+
+#define TRY(expr)                   \
+  do {                              \
+    spg_status s_ = (expr);         \
+    if (s_ != SPG_OK) return s_;    \
+  } while (0)
+
+spg_status status_from_bits(uint32_t bits) {
+  if (bits == 0) return SPG_OK;
+  if (bits & DEV_ERR_INVALID_CSR)
+    return set_error(SPG_ERR_INVALID_CSR,
+                     "input CSR invalid: rowptr must start at 0, be monotone and end at nnz; "
+                     "columns must lie in [0,n) and strictly increase within each row");
+  if (bits & DEV_ERR_HASH_FULL) return set_error(SPG_ERR_HASH_FULL, "a hash table probe ran out");
+  if (bits & DEV_ERR_OVERFLOW)
+    return set_error(SPG_ERR_CUDA, "a row produced more entries than its symbolic count");
+  return set_error(SPG_ERR_CUDA, "device status word 0x%x", bits);
+}
+
+spg_config merged_config(const spg_config* user) {
+  spg_config c{};
+  if (user && user->struct_size >= (int32_t)sizeof(int32_t)) {
+    size_t sz = (size_t)user->struct_size < sizeof(spg_config) ? (size_t)user->struct_size
+                                                               : sizeof(spg_config);
+    std::memcpy(&c, user, sz);
+  }
+  c.struct_size = sizeof(spg_config);
+  if (c.max_smem_slots <= 0) c.max_smem_slots = 8192;
+  if (c.heavy_threads <= 0) c.heavy_threads = 512;
+  if (c.window_bits <= 0) c.window_bits = 1 << 18;
+  return c;
+}
+
+int table_log2_cap(int slots) {
+  int lg = ceil_log2_64(slots < 16 ? 16 : slots);
+  if (lg > kMaxTableLog2) lg = kMaxTableLog2;
+  if ((1 << lg) > slots && lg > kMinTableLog2) --lg;  // largest power of two <= slots
+  return lg;
+}
+
+template <class T>
+spg_status palloc(spg_plan* p, T** out, int64_t count) {
+  size_t bytes = sizeof(T) * (size_t)(count > 0 ? count : 1);
+  void* ptr = nullptr;
+  cudaError_t e = cudaMallocFromPoolAsync(&ptr, bytes, p->ctx->pool, p->stream);
+  if (e != cudaSuccess) return cuda_status(e, "workspace allocation");
+  p->ptrs.push_back(ptr);
+  p->ws_bytes += (int64_t)bytes;
+  *out = (T*)ptr;
+  return SPG_OK;
+}
+
+spg_status check_matrix(const spg_csr_dev* A) {
+  if (!A) return set_error(SPG_ERR_INVALID_ARG, "null matrix");
+  if (A->n < 0 || A->nnz < 0) return set_error(SPG_ERR_INVALID_ARG, "negative n or nnz");
+  if (A->nnz > INT32_MAX)
+    return set_error(SPG_ERR_UNSUPPORTED, "nnz(A) = %lld exceeds int32 row pointers",
+                     (long long)A->nnz);
+  if (!A->rowptr) return set_error(SPG_ERR_INVALID_ARG, "null rowptr");
+  if (A->nnz > 0 && (!A->col || !A->val)) return set_error(SPG_ERR_INVALID_ARG, "null col/val");
+  return SPG_OK;
+}
+
+// Validate A on the device and wait for the verdict (host sync #1).
+spg_status validate_device(spg_ctx* ctx, const MatView& A, cudaStream_t st) {
+  TRY_CUDA(cudaMemsetAsync(ctx->d_status, 0, sizeof(uint32_t), st), "status reset");
+  {
+    ProfScope ps(ctx, "plan/validate", st);
+    TRY_CUDA(launch_validate(A, ctx->d_status, st), "validate");
+  }
+  TRY_CUDA(cudaMemcpyAsync(ctx->h_pin, ctx->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, st),
+           "status readback");
+  TRY_CUDA(cudaStreamSynchronize(st), "validate sync");
+  return status_from_bits(*(uint32_t*)ctx->h_pin);
+}
+
+void plan_free(spg_plan* p) {
+  if (!p) return;
+  if (p->exec_done) {
+    cudaStreamWaitEvent(p->stream, p->exec_done, 0);
+    cudaEventDestroy(p->exec_done);
+  }
+  for (void* ptr : p->ptrs) cudaFreeAsync(ptr, p->stream);
+  delete p;
+}
+
+spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
+  spg_ctx* ctx = p->ctx;
+  cudaStream_t st = p->stream;
+  const int32_t n = Ad->n;
+  const bool gram = p->task == SPG_TASK_AATS;
+  p->n = n;
+  p->A = MatView{n, Ad->nnz, Ad->rowptr, Ad->col, Ad->val};
+  p->info.n = n;
+  p->info.task = p->task;
+  p->info.nnz_a = Ad->nnz;
+  TRY(validate_device(ctx, p->A, st));
+
+  // B = A, or Aᵀ by the counting-sort transpose
+  if (p->task == SPG_TASK_AA) {
+    p->B = p->A;
+  } else {
+    int32_t *bp, *bi;
+    double* bx;
+    TRY(palloc(p, &bp, (int64_t)n + 1));
+    TRY(palloc(p, &bi, Ad->nnz));
+    TRY(palloc(p, &bx, Ad->nnz));
+    TransposeWork w{};
+    void* scan_tmp;
+    TRY(palloc(p, &w.cnt, n));
+    TRY(palloc(p, &w.cursor, n));
+    TRY(palloc(p, (char**)&scan_tmp, (int64_t)scan_tmp_bytes(n)));
+    w.scan_tmp = scan_tmp;
+    TRY(palloc(p, &w.tmp_col, Ad->nnz));
+    TRY(palloc(p, &w.tmp_val, Ad->nnz));
+    TRY(palloc(p, &w.long_list, n));
+    TRY(palloc(p, &w.long_count, 1));
+    w.status = ctx->d_status;
+    ProfScope ps(ctx, "plan/transpose", st);
+    TRY_CUDA(launch_transpose(p->A, bp, bi, bx, w, ctx->num_sms, st), "transpose");
+    p->B = MatView{n, Ad->nnz, bp, bi, bx};
+  }
+
+  // lanes per row in the sub-warp bins: next power of two of B's mean row length
+  if (ctx->cfg.lanes_per_row > 0) {
+    p->G = ctx->cfg.lanes_per_row;
+  } else {
+    double mean = n > 0 ? (double)Ad->nnz / n : 1.0;
+    int g = 4;
+    while (g < 32 && g < mean) g <<= 1;
+    p->G = g;
+  }
+
+  // pre-pass and symbolic binning (host sync #2: bin sizes)
+  TRY(palloc(p, &p->f, n));
+  TRY(palloc(p, &p->lo, n));
+  TRY(palloc(p, &p->hi, n));
+  {
+    ProfScope ps(ctx, "plan/prepass", st);
+    TRY_CUDA(launch_prepass(p->A, p->B, p->f, p->lo, p->hi, st), "prepass");
+  }
+  const int nblocks = (n + kBinRowsPerBlock - 1) / kBinRowsPerBlock;
+  int32_t* hist;
+  int64_t* counts;
+  int32_t* rows_sym;
+  TRY(palloc(p, &hist, (int64_t)kNumBins * (nblocks > 0 ? nblocks : 1)));
+  TRY(palloc(p, &counts, 4 * kNumBins));
+  TRY(palloc(p, &rows_sym, n));
+  const int force = ctx->cfg.force_heavy ? 1 : 0;
+  BinSource bsym{0, n, p->f, p->lo, p->hi, nullptr, nullptr, kMaxTableLog2, force};
+  {
+    ProfScope ps(ctx, "plan/bin_sym", st);
+    TRY_CUDA(launch_bin_rows(bsym, hist, counts, rows_sym, st), "symbolic binning");
+  }
+  int64_t* hp = p->ctx->h_pin;
+  TRY_CUDA(cudaMemcpyAsync(hp, counts, sizeof(int64_t) * 2 * kNumBins, cudaMemcpyDeviceToHost, st),
+           "bin readback");
+  TRY_CUDA(cudaStreamSynchronize(st), "bin sync");
+  int64_t sym_count[kNumBins], sym_start[kNumBins];
+  for (int b = 0; b < kNumBins; ++b) {
+    sym_count[b] = hp[b];
+    sym_start[b] = hp[kNumBins + b];
+  }
+
+  // symbolic phase
+  TRY(palloc(p, &p->rownnz, n));
+  TRY_CUDA(cudaMemsetAsync(p->rownnz, 0, sizeof(int32_t) * (size_t)(n > 0 ? n : 1), st), "memset");
+  if (gram) {
+    TRY(palloc(p, &p->rowlow, n));
+    TRY_CUDA(cudaMemsetAsync(p->rowlow, 0, sizeof(int32_t) * (size_t)(n > 0 ? n : 1), st),
+             "memset");
+  }
+  RowArgs ra{};
+  ra.A = p->A;
+  ra.B = p->B;
+  ra.rownnz = p->rownnz;
+  ra.rowlow = p->rowlow;
+  ra.status = ctx->d_status;
+  int bins_used = 0;
+  for (int b = 1; b <= kNumTableBins; ++b) {
+    if (sym_count[b] == 0) continue;
+    ++bins_used;
+    RowArgs r = ra;
+    r.rows = rows_sym + sym_start[b];
+    r.nrows = (int32_t)sym_count[b];
+    r.G = hash_bin_lanes(b, p->G);
+    ProfScope ps(ctx, "sym/bin", st, b);
+    TRY_CUDA(launch_hash_bin(b, false, gram, r, ctx->num_sms, st), "symbolic");
+  }
+  if (sym_count[kHeavyBin] > 0) {
+    HeavyArgs h{};
+    h.r = ra;
+    h.r.rows = rows_sym + sym_start[kHeavyBin];
+    h.r.nrows = (int32_t)sym_count[kHeavyBin];
+    h.lo = p->lo;
+    h.hi = p->hi;
+    h.window_bits = ctx->cfg.window_bits;
+    ProfScope ps(ctx, "sym/heavy", st);
+    TRY_CUDA(launch_heavy(false, gram, h, ctx->cfg.heavy_threads, ctx->num_sms, st),
+             "symbolic heavy");
+  }
+
+  // C row pointers (and lower-part offsets of the Gram mirror)
+  void* scan_tmp;
+  TRY(palloc(p, (char**)&scan_tmp, (int64_t)scan_tmp_bytes(n)));
+  TRY(palloc(p, &p->rowptr, (int64_t)n + 1));
+  {
+    ProfScope ps(ctx, "plan/scan", st);
+    TRY_CUDA(launch_scan_i32_i64(p->rownnz, p->rowptr, n, scan_tmp, st), "row pointer scan");
+  }
+  if (gram) {
+    void* scan_tmp2;
+    TRY(palloc(p, (char**)&scan_tmp2, (int64_t)scan_tmp_bytes(n)));
+    TRY(palloc(p, &p->lowptr, (int64_t)n + 1));
+    TRY_CUDA(launch_scan_i32_i64(p->rowlow, p->lowptr, n, scan_tmp2, st), "lower scan");
+  }
+
+  // numeric binning by exact counts, stats; host sync #3 (nnz(C))
+  TRY(palloc(p, &p->rows_num, n));
+  const int num_lg = table_log2_cap(ctx->cfg.max_smem_slots);
+  BinSource bnum{1, n, p->f, p->lo, p->hi, p->rownnz, gram ? p->rowlow : nullptr, num_lg, force};
+  {
+    ProfScope ps(ctx, "plan/bin_num", st);
+    TRY_CUDA(launch_bin_rows(bnum, hist, counts + 2 * kNumBins, p->rows_num, st),
+             "numeric binning");
+  }
+  unsigned long long* stats = nullptr;
+  TRY(palloc(p, &stats, 4));
+  TRY_CUDA(launch_row_stats(p->f, p->rownnz, n, stats, st), "row stats");
+  TRY_CUDA(cudaMemcpyAsync(hp, counts + 2 * kNumBins, sizeof(int64_t) * 2 * kNumBins,
+                           cudaMemcpyDeviceToHost, st), "readback");
+  TRY_CUDA(cudaMemcpyAsync(hp + 2 * kNumBins, p->rowptr + n, sizeof(int64_t),
+                           cudaMemcpyDeviceToHost, st), "readback");
+  if (gram)
+    TRY_CUDA(cudaMemcpyAsync(hp + 2 * kNumBins + 1, p->lowptr + n, sizeof(int64_t),
+                             cudaMemcpyDeviceToHost, st), "readback");
+  TRY_CUDA(cudaMemcpyAsync(hp + 2 * kNumBins + 2, stats, sizeof(unsigned long long) * 3,
+                           cudaMemcpyDeviceToHost, st), "readback");
+  TRY_CUDA(cudaMemcpyAsync(hp + 2 * kNumBins + 5, ctx->d_status, sizeof(uint32_t),
+                           cudaMemcpyDeviceToHost, st), "readback");
+  TRY_CUDA(cudaStreamSynchronize(st), "plan sync");
+  TRY(status_from_bits(*(uint32_t*)(hp + 2 * kNumBins + 5)));
+  for (int b = 0; b < kNumBins; ++b) {
+    p->num_count[b] = hp[b];
+    p->num_start[b] = hp[kNumBins + b];
+  }
+  p->nnz_c = n > 0 ? hp[2 * kNumBins] : 0;
+  p->nnz_low = (gram && n > 0) ? hp[2 * kNumBins + 1] : 0;
+  const unsigned long long* sv = (const unsigned long long*)(hp + 2 * kNumBins + 2);
+  p->info.nnz_c = p->nnz_c;
+  p->info.products = (int64_t)sv[0];
+  p->info.products_computed = (int64_t)sv[0];
+  p->info.max_row_products = (int64_t)sv[1];
+  p->info.max_row_nnz = (int64_t)sv[2];
+  p->info.heavy_rows = p->num_count[kHeavyBin];
+  for (int b = 1; b < kNumBins; ++b)
+    if (p->num_count[b] > 0) ++bins_used;
+  p->info.bins_used = bins_used;
+  p->info.output_bytes = 8 * ((int64_t)n + 1) + 12 * p->nnz_c;
+  p->info.workspace_bytes = p->ws_bytes;
+  return SPG_OK;
+}
+
+spg_status execute_impl(spg_plan* p, spg_csr_out* C, cudaStream_t st) {
+  spg_ctx* ctx = p->ctx;
+  const int32_t n = p->n;
+  const bool gram = p->task == SPG_TASK_AATS;
+  if (!C) return set_error(SPG_ERR_INVALID_ARG, "null output");
+  if (C->n != n) return set_error(SPG_ERR_INVALID_ARG, "output n %d != %d", C->n, n);
+  if (!C->rowptr || (p->nnz_c > 0 && (!C->col || !C->val)))
+    return set_error(SPG_ERR_INVALID_ARG, "null output arrays");
+  C->nnz = p->nnz_c;
+  TRY_CUDA(cudaSetDevice(ctx->device), "set device");
+  TRY_CUDA(cudaMemcpyAsync(C->rowptr, p->rowptr, sizeof(int64_t) * ((size_t)n + 1),
+                           cudaMemcpyDeviceToDevice, st), "rowptr copy");
+  std::vector<void*> tmp;
+  auto talloc = [&](void** ptr, size_t bytes) -> spg_status {
+    cudaError_t e = cudaMallocFromPoolAsync(ptr, bytes ? bytes : 1, ctx->pool, st);
+    if (e != cudaSuccess) return cuda_status(e, "execute workspace");
+    tmp.push_back(*ptr);
+    return SPG_OK;
+  };
+  spg_status result = SPG_OK;
+  do {
+    if (p->nnz_c == 0) break;
+    RowArgs ra{};
+    ra.A = p->A;
+    ra.B = p->B;
+    ra.rowptr = p->rowptr;
+    ra.cnt_in = p->rownnz;
+    ra.low_in = p->rowlow;
+    ra.ccol = C->col;
+    ra.cval = C->val;
+    ra.status = ctx->d_status;
+    if (gram) {
+      void *cur, *lc, *lv;
+      if ((result = talloc(&cur, sizeof(int32_t) * (size_t)n)) != SPG_OK) break;
+      if ((result = talloc(&lc, sizeof(int32_t) * (size_t)p->nnz_low)) != SPG_OK) break;
+      if ((result = talloc(&lv, sizeof(double) * (size_t)p->nnz_low)) != SPG_OK) break;
+      cudaError_t e = cudaMemsetAsync(cur, 0, sizeof(int32_t) * (size_t)n, st);
+      if (e != cudaSuccess) { result = cuda_status(e, "memset"); break; }
+      ra.lowptr = p->lowptr;
+      ra.cursor = (int32_t*)cur;
+      ra.lcol = (int32_t*)lc;
+      ra.lval = (double*)lv;
+    }
+    for (int b = 1; b <= kNumTableBins && result == SPG_OK; ++b) {
+      if (p->num_count[b] == 0) continue;
+      RowArgs r = ra;
+      r.rows = p->rows_num + p->num_start[b];
+      r.nrows = (int32_t)p->num_count[b];
+      r.G = hash_bin_lanes(b, p->G);
+      ProfScope ps(ctx, "num/bin", st, b);
+      cudaError_t e = launch_hash_bin(b, true, gram, r, ctx->num_sms, st);
+      if (e != cudaSuccess) result = cuda_status(e, "numeric");
+    }
+    if (result != SPG_OK) break;
+    if (p->num_count[kHeavyBin] > 0) {
+      HeavyArgs h{};
+      h.r = ra;
+      h.r.rows = p->rows_num + p->num_start[kHeavyBin];
+      h.r.nrows = (int32_t)p->num_count[kHeavyBin];
+      h.lo = p->lo;
+      h.hi = p->hi;
+      h.window_bits = ctx->cfg.window_bits;
+      ProfScope ps(ctx, "num/heavy", st);
+      cudaError_t e = launch_heavy(true, gram, h, ctx->cfg.heavy_threads, ctx->num_sms, st);
+      if (e != cudaSuccess) { result = cuda_status(e, "numeric heavy"); break; }
+    }
+    if (gram && p->nnz_low > 0) {
+      void *ll, *lcnt;
+      if ((result = talloc(&ll, sizeof(int32_t) * (size_t)n)) != SPG_OK) break;
+      if ((result = talloc(&lcnt, sizeof(int32_t))) != SPG_OK) break;
+      SegSortArgs sa{};
+      sa.nseg = n;
+      sa.src_off64 = p->lowptr;
+      sa.dst_off64 = p->rowptr;
+      sa.lens = p->rowlow;
+      sa.src_key = ra.lcol;
+      sa.src_val = ra.lval;
+      sa.dst_key = C->col;
+      sa.dst_val = C->val;
+      sa.key_bound = n;
+      sa.long_list = (int32_t*)ll;
+      sa.long_count = (int32_t*)lcnt;
+      sa.status = ctx->d_status;
+      ProfScope ps(ctx, "num/mirror_sort", st);
+      cudaError_t e = launch_segsort(sa, ctx->num_sms, st);
+      if (e != cudaSuccess) { result = cuda_status(e, "mirror sort"); break; }
+    }
+  } while (0);
+  for (void* ptr : tmp) cudaFreeAsync(ptr, st);
+  if (result != SPG_OK) return result;
+  if (!p->exec_done) TRY_CUDA(cudaEventCreateWithFlags(&p->exec_done, cudaEventDisableTiming), "event");
+  TRY_CUDA(cudaEventRecord(p->exec_done, st), "event record");
+  return SPG_OK;
+}
+
+spg_task parse_task(const char* t, bool* ok) {
+  *ok = true;
+  if (t && std::strcmp(t, "AA") == 0) return SPG_TASK_AA;
+  if (t && std::strcmp(t, "AAt") == 0) return SPG_TASK_AAT;
+  if (t && std::strcmp(t, "AAtS") == 0) return SPG_TASK_AATS;
+  *ok = false;
+  return SPG_TASK_AA;
+}
+
+}  // namespace
+
+extern "C" {
+
+spg_status spg_create(spg_ctx** out, const spg_config* cfg) {
+  clear_error();
+  if (!out) return set_error(SPG_ERR_INVALID_ARG, "null context pointer");
+  *out = nullptr;
+  spg_ctx* ctx = new spg_ctx();
+  ctx->cfg = merged_config(cfg);
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    delete ctx;
+    return cuda_status(e, "cudaGetDevice (is a CUDA GPU present?)");
+  }
+  if (cfg && cfg->struct_size > 0 && cfg->device > 0) dev = cfg->device;
+  ctx->device = dev;
+  spg_status st = SPG_OK;
+  do {
+    if ((e = cudaSetDevice(dev)) != cudaSuccess) { st = cuda_status(e, "cudaSetDevice"); break; }
+    if ((e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, dev)) !=
+        cudaSuccess) { st = cuda_status(e, "device attribute"); break; }
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    if ((e = cudaMemPoolCreate(&ctx->pool, &props)) != cudaSuccess) {
+      st = cuda_status(e, "memory pool");
+      break;
+    }
+    uint64_t thr = ctx->cfg.pool_release_bytes > 0 ? (uint64_t)ctx->cfg.pool_release_bytes
+                                                   : UINT64_MAX;
+    cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    if ((e = cudaMalloc(&ctx->d_status, 256)) != cudaSuccess) { st = cuda_status(e, "status"); break; }
+    if ((e = cudaMemset(ctx->d_status, 0, 256)) != cudaSuccess) { st = cuda_status(e, "status"); break; }
+    if ((e = cudaMallocHost(&ctx->h_pin, 512)) != cudaSuccess) { st = cuda_status(e, "pinned"); break; }
+  } while (0);
+  if (st != SPG_OK) {
+    spg_destroy(ctx);
+    return st;
+  }
+  *out = ctx;
+  return SPG_OK;
+}
+
+spg_status spg_destroy(spg_ctx* ctx) {
+  clear_error();
+  if (!ctx) return SPG_OK;
+  cudaSetDevice(ctx->device);
+  cudaDeviceSynchronize();
+  prof_resolve(ctx);
+  for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
+  if (ctx->d_status) cudaFree(ctx->d_status);
+  if (ctx->h_pin) cudaFreeHost(ctx->h_pin);
+  if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
+  delete ctx;
+  return SPG_OK;
+}
+
+spg_status spg_check_device_status(spg_ctx* ctx, void* stream) {
+  clear_error();
+  if (!ctx) return set_error(SPG_ERR_INVALID_ARG, "null context");
+  cudaStream_t st = (cudaStream_t)stream;
+  TRY_CUDA(cudaMemcpyAsync(ctx->h_pin, ctx->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, st),
+           "status readback");
+  TRY_CUDA(cudaStreamSynchronize(st), "status sync");
+  uint32_t bits = *(uint32_t*)ctx->h_pin;
+  TRY_CUDA(cudaMemsetAsync(ctx->d_status, 0, sizeof(uint32_t), st), "status reset");
+  return status_from_bits(bits);
+}
+
+spg_status spg_plan_create(spg_ctx* ctx, spg_task task, const spg_csr_dev* A, void* stream,
+                           spg_plan** out) {
+  clear_error();
+  if (!ctx || !out) return set_error(SPG_ERR_INVALID_ARG, "null context or plan pointer");
+  *out = nullptr;
+  if (task != SPG_TASK_AA && task != SPG_TASK_AAT && task != SPG_TASK_AATS)
+    return set_error(SPG_ERR_INVALID_ARG, "unknown task %d", (int)task);
+  TRY(check_matrix(A));
+  TRY_CUDA(cudaSetDevice(ctx->device), "set device");
+  spg_plan* p = new spg_plan();
+  p->ctx = ctx;
+  p->task = task;
+  p->stream = (cudaStream_t)stream;
+  spg_status st = plan_build(p, A);
+  if (st != SPG_OK) {
+    // keep the message of the failure, then release what was allocated
+    cudaStreamSynchronize(p->stream);
+    plan_free(p);
+    return st;
+  }
+  *out = p;
+  return SPG_OK;
+}
+
+spg_status spg_plan_get_info(const spg_plan* plan, spg_plan_info* info) {
+  clear_error();
+  if (!plan || !info) return set_error(SPG_ERR_INVALID_ARG, "null argument");
+  *info = plan->info;
+  return SPG_OK;
+}
+
+spg_status spg_execute(spg_plan* plan, spg_csr_out* C, void* stream) {
+  clear_error();
+  if (!plan) return set_error(SPG_ERR_INVALID_ARG, "null plan");
+  return execute_impl(plan, C, (cudaStream_t)stream);
+}
+
+spg_status spg_plan_destroy(spg_plan* plan) {
+  clear_error();
+  if (!plan) return SPG_OK;
+  cudaSetDevice(plan->ctx->device);
+  plan_free(plan);
+  return SPG_OK;
+}
+
+spg_status spg_multiply(spg_ctx* ctx, spg_task task, const spg_csr_dev* A, spg_csr_out* C,
+                        void* stream) {
+  clear_error();
+  if (!C) return set_error(SPG_ERR_INVALID_ARG, "null output");
+  spg_plan* p = nullptr;
+  TRY(spg_plan_create(ctx, task, A, stream, &p));
+  cudaStream_t st = (cudaStream_t)stream;
+  const int32_t n = A->n;
+  C->n = n;
+  C->nnz = p->nnz_c;
+  C->rowptr = nullptr;
+  C->col = nullptr;
+  C->val = nullptr;
+  spg_status s = SPG_OK;
+  cudaError_t e = cudaMallocFromPoolAsync((void**)&C->rowptr, sizeof(int64_t) * ((size_t)n + 1),
+                                          ctx->pool, st);
+  if (e == cudaSuccess)
+    e = cudaMallocFromPoolAsync((void**)&C->col, sizeof(int32_t) * (size_t)(p->nnz_c ? p->nnz_c : 1),
+                                ctx->pool, st);
+  if (e == cudaSuccess)
+    e = cudaMallocFromPoolAsync((void**)&C->val, sizeof(double) * (size_t)(p->nnz_c ? p->nnz_c : 1),
+                                ctx->pool, st);
+  if (e != cudaSuccess) s = cuda_status(e, "output allocation");
+  if (s == SPG_OK) s = execute_impl(p, C, st);
+  if (s != SPG_OK) {
+    if (C->rowptr) cudaFreeAsync(C->rowptr, st);
+    if (C->col) cudaFreeAsync(C->col, st);
+    if (C->val) cudaFreeAsync(C->val, st);
+    C->rowptr = nullptr;
+    C->col = nullptr;
+    C->val = nullptr;
+  }
+  plan_free(p);
+  return s;
+}
+
+spg_status spg_free(spg_ctx* ctx, void* dev_ptr, void* stream) {
+  clear_error();
+  if (!ctx) return set_error(SPG_ERR_INVALID_ARG, "null context");
+  if (!dev_ptr) return SPG_OK;
+  TRY_CUDA(cudaFreeAsync(dev_ptr, (cudaStream_t)stream), "free");
+  return SPG_OK;
+}
+
+spg_status spg_transpose(spg_ctx* ctx, const spg_csr_dev* A, int32_t* t_rowptr, int32_t* t_col,
+                         double* t_val, void* stream) {
+  clear_error();
+  if (!ctx) return set_error(SPG_ERR_INVALID_ARG, "null context");
+  TRY(check_matrix(A));
+  if (!t_rowptr || (A->nnz > 0 && (!t_col || !t_val)))
+    return set_error(SPG_ERR_INVALID_ARG, "null output arrays");
+  TRY_CUDA(cudaSetDevice(ctx->device), "set device");
+  spg_plan tmp;  // borrow the plan allocator for the workspace
+  tmp.ctx = ctx;
+  tmp.stream = (cudaStream_t)stream;
+  const int32_t n = A->n;
+  MatView Av{n, A->nnz, A->rowptr, A->col, A->val};
+  spg_status st = validate_device(ctx, Av, tmp.stream);
+  TransposeWork w{};
+  void* scan_tmp = nullptr;
+  if (st == SPG_OK) st = palloc(&tmp, &w.cnt, n);
+  if (st == SPG_OK) st = palloc(&tmp, &w.cursor, n);
+  if (st == SPG_OK) st = palloc(&tmp, (char**)&scan_tmp, (int64_t)scan_tmp_bytes(n));
+  if (st == SPG_OK) st = palloc(&tmp, &w.tmp_col, A->nnz);
+  if (st == SPG_OK) st = palloc(&tmp, &w.tmp_val, A->nnz);
+  if (st == SPG_OK) st = palloc(&tmp, &w.long_list, n);
+  if (st == SPG_OK) st = palloc(&tmp, &w.long_count, 1);
+  w.scan_tmp = scan_tmp;
+  w.status = ctx->d_status;
+  if (st == SPG_OK) {
+    cudaError_t e = launch_transpose(Av, t_rowptr, t_col, t_val, w, ctx->num_sms, tmp.stream);
+    if (e != cudaSuccess) st = cuda_status(e, "transpose");
+  }
+  for (void* ptr : tmp.ptrs) cudaFreeAsync(ptr, tmp.stream);
+  tmp.ptrs.clear();
+  return st;
+}
+
+spg_status spg_describe(spg_ctx* ctx, const spg_csr_dev* A, spg_descriptors* d, void* stream) {
+  clear_error();
+  if (!ctx || !d) return set_error(SPG_ERR_INVALID_ARG, "null argument");
+  TRY(check_matrix(A));
+  TRY_CUDA(cudaSetDevice(ctx->device), "set device");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int32_t n = A->n;
+  MatView Av{n, A->nnz, A->rowptr, A->col, A->val};
+  TRY(validate_device(ctx, Av, st));
+  spg_plan tmp;
+  tmp.ctx = ctx;
+  tmp.stream = st;
+  int32_t* cc = nullptr;
+  DescAccum* acc = nullptr;
+  spg_status s = palloc(&tmp, &cc, n);
+  if (s == SPG_OK) s = palloc(&tmp, &acc, 1);
+  if (s == SPG_OK) {
+    cudaError_t e = cudaMemsetAsync(cc, 0, sizeof(int32_t) * (size_t)(n > 0 ? n : 1), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(acc, 0, sizeof(DescAccum), st);
+    if (e == cudaSuccess) e = launch_col_count(Av, cc, st);
+    if (e == cudaSuccess) e = launch_describe(Av, cc, acc, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(ctx->h_pin, acc, sizeof(DescAccum), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) s = cuda_status(e, "describe");
+  }
+  for (void* ptr : tmp.ptrs) cudaFreeAsync(ptr, st);
+  tmp.ptrs.clear();
+  if (s != SPG_OK) return s;
+  DescAccum h;
+  std::memcpy(&h, ctx->h_pin, sizeof(h));
+  std::memset(d, 0, sizeof(*d));
+  d->n = n;
+  d->nnz = A->nnz;
+  const double nn = n > 0 ? (double)n : 1.0;
+  const double nz = A->nnz > 0 ? (double)A->nnz : 1.0;
+  d->mean_deg = (double)A->nnz / nn;
+  const double var = (double)h.sum_deg2 / nn - d->mean_deg * d->mean_deg;
+  d->deg_cv = std::sqrt(var > 0 ? var : 0.0) / (d->mean_deg > 1e-9 ? d->mean_deg : 1e-9);
+  d->products_aa = (int64_t)h.prod_aa;
+  d->products_aat = (int64_t)h.prod_aat;
+  d->fill_aa = (double)h.prod_aa / nz;
+  d->fill_aat = (double)h.prod_aat / nz;
+  d->max_deg = h.max_deg;
+  d->max_col_deg = h.max_col_deg;
+  d->bandwidth = h.bandwidth;
+  d->pattern_symmetry = A->nnz > 0 ? (double)h.sym_hits / nz : 1.0;
+  return SPG_OK;
+}
+
+spg_status spg_profile_enable(spg_ctx* ctx, int32_t enable) {
+  clear_error();
+  if (!ctx) return set_error(SPG_ERR_INVALID_ARG, "null context");
+  ctx->prof = enable != 0;
+  return SPG_OK;
+}
+
+spg_status spg_profile_reset(spg_ctx* ctx) {
+  clear_error();
+  if (!ctx) return set_error(SPG_ERR_INVALID_ARG, "null context");
+  TRY_CUDA(cudaSetDevice(ctx->device), "set device");
+  prof_resolve(ctx);
+  ctx->prof_acc.clear();
+  ctx->launch_base = g_kernel_launches;
+  return SPG_OK;
+}
+
+spg_status spg_profile_read(spg_ctx* ctx, char* json, size_t capacity) {
+  clear_error();
+  if (!ctx || !json || capacity == 0) return set_error(SPG_ERR_INVALID_ARG, "bad arguments");
+  TRY_CUDA(cudaSetDevice(ctx->device), "set device");
+  TRY_CUDA(cudaDeviceSynchronize(), "profile sync");
+  prof_resolve(ctx);
+  std::string out = "{\"launches\": " + std::to_string(g_kernel_launches - ctx->launch_base) +
+                    ", \"kernels\": {";
+  bool first = true;
+  char buf[160];
+  for (const auto& kv : ctx->prof_acc) {
+    std::snprintf(buf, sizeof(buf), "%s\"%s\": {\"count\": %lld, \"ms\": %.6f}", first ? "" : ", ",
+                  kv.first.c_str(), kv.second.second, kv.second.first);
+    out += buf;
+    first = false;
+  }
+  out += "}}";
+  if (out.size() + 1 > capacity)
+    return set_error(SPG_ERR_INVALID_ARG, "profile text needs %zu bytes", out.size() + 1);
+  std::memcpy(json, out.c_str(), out.size() + 1);
+  return SPG_OK;
+}
+
+spg_status spg_checksum(const double* dev_val, int64_t count, double* s, double* as, double* sq) {
+  clear_error();
+  if (!s || !as || !sq || count < 0 || (count > 0 && !dev_val))
+    return set_error(SPG_ERR_INVALID_ARG, "bad checksum arguments");
+  std::vector<double> h((size_t)count);
+  if (count > 0)
+    TRY_CUDA(cudaMemcpy(h.data(), dev_val, sizeof(double) * (size_t)count, cudaMemcpyDeviceToHost),
+             "checksum copy");
+  double a = 0, b = 0, c = 0;
+  for (double x : h) {
+    a += x;
+    b += x < 0 ? -x : x;
+    c += x * x;
+  }
+  *s = a;
+  *as = b;
+  *sq = c;
+  return SPG_OK;
+}
+
+spg_status spg_run_ours(const char* task, const int32_t* dOff, const int32_t* dCol,
+                        const double* dVal, int32_t n, int64_t nnz, int32_t reps,
+                        spg_eng_result* out) {
+  clear_error();
+  bool ok;
+  spg_task t = parse_task(task, &ok);
+  if (!ok) return set_error(SPG_ERR_INVALID_ARG, "task must be AA, AAt or AAtS");
+  if (!out || reps < 0) return set_error(SPG_ERR_INVALID_ARG, "bad arguments");
+  static thread_local spg_ctx* ctx = nullptr;
+  static thread_local int ctx_dev = -1;
+  int dev = 0;
+  TRY_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
+  if (!ctx || ctx_dev != dev) {
+    if (ctx) spg_destroy(ctx);
+    ctx = nullptr;
+    TRY(spg_create(&ctx, nullptr));
+    ctx_dev = dev;
+  }
+  spg_csr_dev A{n, nnz, dOff, dCol, dVal};
+  spg_csr_out C{};
+  // one checked call
+  TRY(spg_multiply(ctx, t, &A, &C, nullptr));
+  double s = 0, as = 0, sq = 0;
+  spg_status st = spg_checksum(C.val, C.nnz, &s, &as, &sq);
+  const int64_t nnz_c = C.nnz;
+  spg_free(ctx, C.rowptr, nullptr);
+  spg_free(ctx, C.col, nullptr);
+  spg_free(ctx, C.val, nullptr);
+  if (st != SPG_OK) return st;
+  TRY_CUDA(cudaDeviceSynchronize(), "sync");
+  float ms = 0.f;
+  if (reps > 0) {
+    cudaEvent_t e0, e1;
+    TRY_CUDA(cudaEventCreate(&e0), "event");
+    TRY_CUDA(cudaEventCreate(&e1), "event");
+    cudaEventRecord(e0, nullptr);
+    for (int r = 0; r < reps && st == SPG_OK; ++r) {
+      spg_csr_out Cr{};
+      st = spg_multiply(ctx, t, &A, &Cr, nullptr);
+      if (st == SPG_OK) {
+        spg_free(ctx, Cr.rowptr, nullptr);
+        spg_free(ctx, Cr.col, nullptr);
+        spg_free(ctx, Cr.val, nullptr);
+      }
+    }
+    cudaEventRecord(e1, nullptr);
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ms /= (float)reps;
+  }
+  if (st != SPG_OK) return st;
+  out->ms = ms;
+  out->nnz = nnz_c;
+  out->s = s;
+  out->as = as;
+  out->sq = sq;
+  return SPG_OK;
+}
+
+}  // extern "C"

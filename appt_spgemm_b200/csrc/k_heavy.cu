@@ -1,0 +1,235 @@
+// Heavy rows: one CTA per row over dense column windows.
+//
+// A row whose table would not fit in shared memory is processed window by
+// window over its output column span [lo, hi]: a shared bitmap of W bits marks
+// the columns hit in [w0, w0+W).  The symbolic phase counts the bits.  The
+// numeric phase turns the bitmap into per-word prefix counts, so a column's
+// rank inside the row is prefix[word] + popc(bits below it): the row's column
+// indices are written in sorted order straight into their CSR slots, values
+// are zeroed there and then accumulated in place, walking row i of A in order
+// with a CTA barrier per k (the same k-ordered, product-rounded sum as the
+// shared-table rows and the CPU oracle).  No global hash table and no sort
+// are needed: the bitmap rank is a counting sort with one bit per key.
+//
+// In the reference every row above 767 products went to a per-row global hash
+// arena of next_pow2(4f/3+1) slots (src/spgemm_engine.cuh:51-57, :79, :101)
+// followed by the global radix sort.
+#include "kernels.h"
+
+namespace spg {
+
+constexpr size_t kHeavyScratch = 256;
+
+size_t heavy_smem_bytes(bool numeric, int threads, int window_bits) {
+  const size_t words = (size_t)window_bits / 32;
+  size_t b = words * 4 + (size_t)threads * 8 + kHeavyScratch;
+  if (numeric) b += words * 4 + (size_t)threads * 8;
+  return b;
+}
+
+// Mark the columns of row `row` that fall in [w0, w0 + 32·nwords) (and, for
+// the Gram upper part, are >= row) in the shared bitmap.  Products are
+// enumerated flat over chunks of blockDim entries of A's row.
+__device__ __forceinline__ void mark_window(const RowArgs& a, int row, long long w0, int nwords,
+                                            uint32_t* bm, int* st_bs, int* st_ex, void* scratch) {
+  const int32_t ps = a.A.rowptr[row], pe = a.A.rowptr[row + 1];
+  const long long wbits = (long long)nwords * 32;
+  for (int32_t pb = ps; pb < pe; pb += blockDim.x) {
+    const int cnt = min((int)blockDim.x, pe - pb);
+    int bs = 0, len = 0;
+    if ((int)threadIdx.x < cnt) {
+      const int32_t k = a.A.col[pb + threadIdx.x];
+      bs = a.B.rowptr[k];
+      len = a.B.rowptr[k + 1] - bs;
+    }
+    int tot;
+    const int ex = block_exclusive_scan(len, (int*)scratch, &tot);
+    st_bs[threadIdx.x] = bs;
+    st_ex[threadIdx.x] = ex;
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
+      int l = 0, h = cnt - 1;  // largest t with st_ex[t] <= idx
+      while (l < h) {
+        const int mid = (l + h + 1) >> 1;
+        if (st_ex[mid] <= idx) l = mid; else h = mid - 1;
+      }
+      const long long d = (long long)a.B.col[st_bs[l] + idx - st_ex[l]] - w0;
+      if (d >= 0 && d < wbits) atomicOr(&bm[d >> 5], 1u << (d & 31));
+    }
+    __syncthreads();
+  }
+}
+
+template <bool GRAM>
+__global__ void __launch_bounds__(1024) k_heavy_sym(HeavyArgs h) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const RowArgs& a = h.r;
+  const int nw_max = h.window_bits / 32;
+  uint32_t* bm = (uint32_t*)smem;
+  int* st_bs = (int*)(bm + nw_max);
+  int* st_ex = st_bs + blockDim.x;
+  void* scratch = (void*)(st_ex + blockDim.x);
+  for (int r = blockIdx.x; r < a.nrows; r += gridDim.x) {
+    const int row = a.rows[r];
+    const int lo = h.lo[row], hi = h.hi[row];
+    long long c = 0, cl = 0;
+    for (long long w0 = lo; w0 <= hi; w0 += h.window_bits) {
+      const int nwords = (int)min((long long)nw_max, (hi - w0) / 32 + 1);
+      for (int i = threadIdx.x; i < nwords; i += blockDim.x) bm[i] = 0u;
+      __syncthreads();
+      mark_window(a, row, w0, nwords, bm, st_bs, st_ex, scratch);
+      int lc = 0, lcl = 0;
+      for (int i = threadIdx.x; i < nwords; i += blockDim.x) {
+        const uint32_t wd = bm[i];
+        lc += __popc(wd);
+        if (GRAM) {
+          const long long c0 = w0 + 32LL * i;
+          if (c0 + 32 <= row) lcl += __popc(wd);
+          else if (c0 < row) lcl += __popc(wd & ((1u << (unsigned)(row - c0)) - 1u));
+        }
+      }
+      c += block_sum64(lc, (long long*)scratch);
+      if (GRAM) cl += block_sum64(lcl, (long long*)scratch);
+    }
+    if (threadIdx.x == 0) {
+      a.rownnz[row] = (int)c;
+      if (GRAM) a.rowlow[row] = (int)cl;
+    }
+    __syncthreads();
+  }
+}
+
+template <bool GRAM>
+__global__ void __launch_bounds__(1024) k_heavy_num(HeavyArgs h) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const RowArgs& a = h.r;
+  const int nw_max = h.window_bits / 32;
+  const int HT = blockDim.x;
+  uint32_t* bm = (uint32_t*)smem;
+  int* pre = (int*)(bm + nw_max);
+  double* st_a = (double*)(pre + nw_max);
+  int* st_bs = (int*)(st_a + HT);
+  int* st_ex = st_bs + HT;
+  void* scratch = (void*)(st_ex + HT);
+  for (int r = blockIdx.x; r < a.nrows; r += gridDim.x) {
+    const int row = a.rows[r];
+    const int hi = h.hi[row];
+    const int lo = GRAM ? max(h.lo[row], row) : h.lo[row];
+    const int32_t low = GRAM ? a.low_in[row] : 0;
+    const long long expect = (long long)a.cnt_in[row] - low;
+    const int64_t base = a.rowptr[row] + low;
+    long long written = 0;
+    for (long long w0 = lo; w0 <= hi; w0 += h.window_bits) {
+      const int nwords = (int)min((long long)nw_max, (hi - w0) / 32 + 1);
+      for (int i = threadIdx.x; i < nwords; i += HT) bm[i] = 0u;
+      __syncthreads();
+      mark_window(a, row, w0, nwords, bm, st_bs, st_ex, scratch);
+      // per-word exclusive prefix of the bit counts
+      const int per = (nwords + HT - 1) / HT;
+      const int wb = min(nwords, (int)threadIdx.x * per), we = min(nwords, wb + per);
+      int local = 0;
+      for (int i = wb; i < we; ++i) local += __popc(bm[i]);
+      int tot;
+      int run = block_exclusive_scan(local, (int*)scratch, &tot);
+      for (int i = wb; i < we; ++i) {
+        pre[i] = run;
+        run += __popc(bm[i]);
+      }
+      // sorted column indices and zeroed values into the row's CSR slots
+      for (int i = wb; i < we; ++i) {
+        uint32_t wd = bm[i];
+        int rk = pre[i];
+        while (wd) {
+          const int b = __ffs(wd) - 1;
+          wd &= wd - 1u;
+          const long long pos = written + rk;
+          if (pos < expect) {
+            a.ccol[base + pos] = (int32_t)(w0 + 32LL * i + b);
+            a.cval[base + pos] = 0.0;
+          }
+          ++rk;
+        }
+      }
+      __syncthreads();
+      // k-ordered accumulation in place
+      const int32_t ps = a.A.rowptr[row], pe = a.A.rowptr[row + 1];
+      const long long wbits = (long long)nwords * 32;
+      for (int32_t pb = ps; pb < pe; pb += HT) {
+        const int cnt = min(HT, pe - pb);
+        if ((int)threadIdx.x < cnt) {
+          const int32_t k = a.A.col[pb + threadIdx.x];
+          const int32_t bs = a.B.rowptr[k];
+          st_bs[threadIdx.x] = bs;
+          st_ex[threadIdx.x] = a.B.rowptr[k + 1] - bs;
+          st_a[threadIdx.x] = a.A.val[pb + threadIdx.x];
+        }
+        __syncthreads();
+        for (int t = 0; t < cnt; ++t) {
+          const int32_t bs = st_bs[t], len = st_ex[t];
+          const double av = st_a[t];
+          for (int q = threadIdx.x; q < len; q += HT) {
+            const long long d = (long long)a.B.col[bs + q] - w0;
+            if (d >= 0 && d < wbits) {
+              const int i = (int)(d >> 5), b = (int)(d & 31);
+              const long long pos = written + pre[i] + __popc(bm[i] & ((1u << b) - 1u));
+              if (pos < expect)
+                a.cval[base + pos] = __dadd_rn(a.cval[base + pos], __dmul_rn(av, a.B.val[bs + q]));
+            }
+          }
+          __syncthreads();
+        }
+      }
+      written += tot;
+    }
+    if (written != expect && threadIdx.x == 0) report(a.status, DEV_ERR_OVERFLOW);
+    if (GRAM) {
+      const long long m = written < expect ? written : expect;
+      for (long long t = threadIdx.x; t < m; t += HT) {
+        const int j = a.ccol[base + t];
+        if (j > row) {
+          const int pos = atomicAdd(&a.cursor[j], 1);
+          if (pos < a.low_in[j]) {
+            const int64_t d = a.lowptr[j] + pos;
+            a.lcol[d] = row;
+            a.lval[d] = a.cval[base + t];
+          } else {
+            report(a.status, DEV_ERR_OVERFLOW);
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <typename K>
+static cudaError_t launch_h(K kernel, int threads, size_t smem, const HeavyArgs& h, int num_sms,
+                            cudaStream_t s) {
+  cudaError_t e;
+  if (smem > 48 * 1024) {
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) per_sm = 1;
+  int64_t grid = (int64_t)per_sm * num_sms;
+  if (grid > h.r.nrows) grid = h.r.nrows;
+  kernel<<<(unsigned)grid, threads, smem, s>>>(h);
+  SPG_COUNT_LAUNCH();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_heavy(bool numeric, bool gram, const HeavyArgs& h, int threads, int num_sms,
+                         cudaStream_t s) {
+  if (h.r.nrows <= 0) return cudaSuccess;
+  const size_t smem = heavy_smem_bytes(numeric, threads, h.window_bits);
+  if (numeric)
+    return gram ? launch_h(k_heavy_num<true>, threads, smem, h, num_sms, s)
+                : launch_h(k_heavy_num<false>, threads, smem, h, num_sms, s);
+  return gram ? launch_h(k_heavy_sym<true>, threads, smem, h, num_sms, s)
+              : launch_h(k_heavy_sym<false>, threads, smem, h, num_sms, s);
+}
+
+}  // namespace spg

@@ -1,0 +1,293 @@
+// Shared-memory hash rows: the symbolic and numeric phases for every row whose
+// table fits in shared memory, one kernel per table-size bin.
+//
+// Replaces k_symbolic / k_numeric (src/spgemm_engine.cuh:71-115), which ran one
+// warp per row over one fixed 1024-slot slice, inserted with atomicCAS on every
+// probe, accumulated with atomicAdd(double) in arbitrary order and emitted
+// (row·n+col, value) pairs in hash order for a global radix sort.  Here:
+//  - the table is sized per bin and the group of lanes per row is sized with it
+//    (sub-warp groups for small tables, a whole CTA for the largest);
+//  - probes read first and CAS only empty slots;
+//  - the numeric phase walks row i of A in order and synchronises the group
+//    after each k, so every output value is Σ_k a_ik·b_kj added in increasing
+//    position of k with the product rounded first — the same sum the CPU
+//    oracle forms, bit for bit;
+//  - the row is compacted and bitonic-sorted in shared memory and written to
+//    its final CSR slots, so no global sort exists.
+#include <climits>
+
+#include "kernels.h"
+
+namespace spg {
+
+__host__ __device__ constexpr size_t row_group_bytes(int T, int G, bool numeric) {
+  return numeric ? (size_t)T * 12 + (size_t)G * 16 : (size_t)T * 4 + (size_t)G * 8;
+}
+constexpr size_t kCtaScratchBytes = 256;  // 32 long longs for block reductions
+
+__device__ __forceinline__ int grp_sum(const WarpGroup& g, int v, void*) { return g.sum(v); }
+__device__ __forceinline__ int grp_sum(const CtaGroup&, int v, void* scratch) {
+  return (int)block_sum64(v, (long long*)scratch);
+}
+
+// Move the occupied slots of keys/vals[0..T) to the front in slot order.
+template <int T>
+__device__ __forceinline__ int grp_compact(const WarpGroup& g, int* keys, double* vals, void*) {
+  int m = 0;
+  for (int base = 0; base < T; base += g.G) {
+    const int s = base + g.lane;
+    const int key = keys[s];
+    const double v = vals[s];
+    const bool occ = key != kEmptyKey;
+    const unsigned bal = g.ballot(occ);
+    const int pos = m + __popc(bal & ((1u << g.lane) - 1u));
+    g.sync();
+    if (occ) {
+      keys[pos] = key;
+      vals[pos] = v;
+    }
+    m += __popc(bal);
+    g.sync();
+  }
+  return m;
+}
+
+template <int T>
+__device__ __forceinline__ int grp_compact(const CtaGroup& g, int* keys, double* vals,
+                                           void* scratch) {
+  int m = 0;
+  for (int base = 0; base < T; base += g.G) {
+    const int s = base + g.lane;
+    int key = kEmptyKey;
+    double v = 0.0;
+    if (s < T) {
+      key = keys[s];
+      v = vals[s];
+    }
+    const bool occ = key != kEmptyKey;
+    int tot;
+    const int ex = block_exclusive_scan(occ ? 1 : 0, (int*)scratch, &tot);
+    // writes land below base + G; the next chunk reads only slots >= base + G
+    if (occ) {
+      keys[m + ex] = key;
+      vals[m + ex] = v;
+    }
+    m += tot;
+  }
+  __syncthreads();
+  return m;
+}
+
+template <int LOG2T, bool NUMERIC, bool GRAM, class Grp>
+__device__ __forceinline__ void hash_row(const Grp& g, const RowArgs& a, const int row,
+                                         int* __restrict__ keys, double* __restrict__ vals,
+                                         int* st_bs, int* st_len, double* st_a, void* scratch) {
+  constexpr int T = 1 << LOG2T;
+  for (int s = g.lane; s < T; s += g.G) {
+    keys[s] = kEmptyKey;
+    if (NUMERIC) vals[s] = 0.0;
+  }
+  const int32_t ps = a.A.rowptr[row], pe = a.A.rowptr[row + 1];
+  for (int32_t pb = ps; pb < pe; pb += g.G) {
+    const int cnt = min(g.G, pe - pb);
+    g.sync();  // table cleared / previous chunk's staging consumed
+    if (g.lane < cnt) {
+      const int32_t k = a.A.col[pb + g.lane];
+      const int32_t bs = a.B.rowptr[k];
+      st_bs[g.lane] = bs;
+      st_len[g.lane] = a.B.rowptr[k + 1] - bs;
+      if (NUMERIC) st_a[g.lane] = a.A.val[pb + g.lane];
+    }
+    g.sync();
+    for (int t = 0; t < cnt; ++t) {
+      const int32_t bs = st_bs[t], len = st_len[t];
+      const double av = NUMERIC ? st_a[t] : 0.0;
+      for (int q = g.lane; q < len; q += g.G) {
+        const int32_t j = a.B.col[bs + q];
+        if (NUMERIC && GRAM && j < row) continue;
+        const int slot = hash_insert<LOG2T>(keys, j, a.status);
+        if (NUMERIC && slot >= 0)
+          vals[slot] = __dadd_rn(vals[slot], __dmul_rn(av, a.B.val[bs + q]));
+      }
+      if (NUMERIC) g.sync();  // k-order of the accumulation
+    }
+  }
+  g.sync();
+
+  if (!NUMERIC) {
+    int c = 0, cl = 0;
+    for (int s = g.lane; s < T; s += g.G) {
+      const int k = keys[s];
+      if (k != kEmptyKey) {
+        ++c;
+        if (GRAM && k < row) ++cl;
+      }
+    }
+    c = grp_sum(g, c, scratch);
+    if (GRAM) cl = grp_sum(g, cl, scratch);
+    if (g.lane == 0) {
+      a.rownnz[row] = c;
+      if (GRAM) a.rowlow[row] = cl;
+    }
+    g.sync();
+    return;
+  }
+
+  int m = grp_compact<T>(g, keys, vals, scratch);
+  const int P = next_pow2_int(m);
+  for (int s = m + g.lane; s < P; s += g.G) keys[s] = INT_MAX;
+  g.sync();
+  bitonic_sort_pairs(g, keys, vals, P);
+
+  const int32_t low = GRAM ? a.low_in[row] : 0;
+  const int expect = a.cnt_in[row] - low;
+  if (m != expect) {
+    if (g.lane == 0) report(a.status, DEV_ERR_OVERFLOW);
+    if (m > expect) m = expect;
+  }
+  const int64_t base = a.rowptr[row] + low;
+  for (int t = g.lane; t < m; t += g.G) {
+    const int j = keys[t];
+    const double v = vals[t];
+    a.ccol[base + t] = j;
+    a.cval[base + t] = v;
+    if (GRAM && j > row) {
+      const int pos = atomicAdd(&a.cursor[j], 1);
+      if (pos < a.low_in[j]) {
+        const int64_t d = a.lowptr[j] + pos;
+        a.lcol[d] = row;
+        a.lval[d] = v;
+      } else {
+        report(a.status, DEV_ERR_OVERFLOW);
+      }
+    }
+  }
+  g.sync();  // the table is reused by the group's next row
+}
+
+template <int LOG2T, bool NUMERIC, bool GRAM>
+__global__ void __launch_bounds__(256) k_hash_warp(RowArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  constexpr int T = 1 << LOG2T;
+  const WarpGroup g(a.G);
+  const int rows_per_cta = blockDim.x / a.G;
+  const int gi = threadIdx.x / a.G;
+  unsigned char* base = smem + (size_t)gi * row_group_bytes(T, a.G, NUMERIC);
+  double* vals = (double*)base;
+  int *keys, *st_bs, *st_len;
+  double* st_a = nullptr;
+  if (NUMERIC) {
+    keys = (int*)(base + (size_t)T * 8);
+    st_a = (double*)(base + (size_t)T * 12);
+    st_bs = (int*)(base + (size_t)T * 12 + (size_t)a.G * 8);
+  } else {
+    keys = (int*)base;
+    st_bs = keys + T;
+  }
+  st_len = st_bs + a.G;
+  for (int r = blockIdx.x * rows_per_cta + gi; r < a.nrows; r += gridDim.x * rows_per_cta)
+    hash_row<LOG2T, NUMERIC, GRAM>(g, a, a.rows[r], keys, vals, st_bs, st_len, st_a, nullptr);
+}
+
+template <int LOG2T, bool NUMERIC, bool GRAM>
+__global__ void __launch_bounds__(1024) k_hash_cta(RowArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  constexpr int T = 1 << LOG2T;
+  const CtaGroup g;
+  const int G = blockDim.x;
+  unsigned char* p = smem;
+  double* vals = (double*)p;
+  if (NUMERIC) p += (size_t)T * 8;
+  int* keys = (int*)p;
+  p += (size_t)T * 4;
+  double* st_a = (double*)p;
+  if (NUMERIC) p += (size_t)G * 8;
+  int* st_bs = (int*)p;
+  int* st_len = st_bs + G;
+  void* scratch = (void*)(p + (size_t)G * 8);
+  for (int r = blockIdx.x; r < a.nrows; r += gridDim.x)
+    hash_row<LOG2T, NUMERIC, GRAM>(g, a, a.rows[r], keys, vals, st_bs, st_len, st_a, scratch);
+}
+
+int hash_bin_lanes(int bin, int lanes_cfg) {
+  const int lg = bin + kMinTableLog2 - 1;
+  const int T = 1 << lg;
+  if (lg >= 11) return T / 16;  // one row per CTA: 128 … 1024 threads
+  int G = lanes_cfg > T / 8 ? lanes_cfg : T / 8;
+  if (G > 32) G = 32;
+  if (G > T) G = T;
+  if (G < 1) G = 1;
+  return G;
+}
+
+template <typename K>
+static cudaError_t launch_kernel(K kernel, int threads, size_t smem, int nwork_ctas, int num_sms,
+                                 const RowArgs& a, cudaStream_t s) {
+  cudaError_t e;
+  if (smem > 48 * 1024) {
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) per_sm = 1;
+  int64_t grid = (int64_t)per_sm * num_sms;
+  if (grid > nwork_ctas) grid = nwork_ctas;
+  if (grid < 1) grid = 1;
+  kernel<<<(unsigned)grid, threads, smem, s>>>(a);
+  SPG_COUNT_LAUNCH();
+  return cudaGetLastError();
+}
+
+template <int LOG2T, bool NUMERIC, bool GRAM>
+static cudaError_t launch_lg(const RowArgs& a, int num_sms, cudaStream_t s) {
+  constexpr int T = 1 << LOG2T;
+  if (LOG2T >= 11) {
+    const int threads = T / 16;
+    const size_t smem = row_group_bytes(T, threads, NUMERIC) + kCtaScratchBytes;
+    return launch_kernel(k_hash_cta<LOG2T, NUMERIC, GRAM>, threads, smem, a.nrows, num_sms, a, s);
+  }
+  const int G = a.G;
+  const size_t per = row_group_bytes(T, G, NUMERIC);
+  const int unit = 32 / G;  // rows per warp
+  int rows = 256 / G;
+  const size_t budget = 48 * 1024;
+  int by_smem = (int)(budget / per);
+  by_smem = (by_smem / unit) * unit;
+  if (by_smem < unit) by_smem = unit;
+  if (rows > by_smem) rows = by_smem;
+  const int threads = rows * G;
+  const size_t smem = per * rows;
+  const int nwork = (a.nrows + rows - 1) / rows;
+  return launch_kernel(k_hash_warp<LOG2T, NUMERIC, GRAM>, threads, smem, nwork, num_sms, a, s);
+}
+
+template <bool NUMERIC, bool GRAM>
+static cudaError_t launch_mode(int bin, const RowArgs& a, int num_sms, cudaStream_t s) {
+  switch (bin + kMinTableLog2 - 1) {
+    case 4: return launch_lg<4, NUMERIC, GRAM>(a, num_sms, s);
+    case 5: return launch_lg<5, NUMERIC, GRAM>(a, num_sms, s);
+    case 6: return launch_lg<6, NUMERIC, GRAM>(a, num_sms, s);
+    case 7: return launch_lg<7, NUMERIC, GRAM>(a, num_sms, s);
+    case 8: return launch_lg<8, NUMERIC, GRAM>(a, num_sms, s);
+    case 9: return launch_lg<9, NUMERIC, GRAM>(a, num_sms, s);
+    case 10: return launch_lg<10, NUMERIC, GRAM>(a, num_sms, s);
+    case 11: return launch_lg<11, NUMERIC, GRAM>(a, num_sms, s);
+    case 12: return launch_lg<12, NUMERIC, GRAM>(a, num_sms, s);
+    case 13: return launch_lg<13, NUMERIC, GRAM>(a, num_sms, s);
+    case 14: return launch_lg<14, NUMERIC, GRAM>(a, num_sms, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_hash_bin(int bin, bool numeric, bool gram, const RowArgs& a, int num_sms,
+                            cudaStream_t s) {
+  if (a.nrows <= 0) return cudaSuccess;
+  if (numeric) return gram ? launch_mode<true, true>(bin, a, num_sms, s)
+                           : launch_mode<true, false>(bin, a, num_sms, s);
+  return gram ? launch_mode<false, true>(bin, a, num_sms, s)
+              : launch_mode<false, false>(bin, a, num_sms, s);
+}
+
+}  // namespace spg

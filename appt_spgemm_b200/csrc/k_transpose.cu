@@ -1,0 +1,234 @@
+// CSR → CSR-of-Aᵀ by counting sort, and the segment sort it (and the Gram
+// mirror) finishes with.
+//
+// The reference builds Aᵀ with a global atomicAdd histogram, a Thrust scan and
+// a one-thread-per-row atomic-cursor scatter (k_colcount / k_scatter /
+// build_At, src/spgemm_engine.cuh:37-44, :140-146), which leaves the entries of
+// each Aᵀ row in a run-dependent order.  Here the scatter is one warp per row
+// (coalesced reads of A) into a staging copy, and a segment sort then orders
+// every Aᵀ row by its row index into the final arrays, so the transpose is
+// deterministic and its rows are sorted like cusparseCsr2cscEx2's.
+#include <climits>
+
+#include "kernels.h"
+
+namespace spg {
+
+__global__ void k_transpose_scatter(MatView A, const int32_t* __restrict__ t_rowptr,
+                                    int32_t* __restrict__ cursor, int32_t* __restrict__ tmp_col,
+                                    double* __restrict__ tmp_val) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t i = warp; i < A.n; i += nwarps) {
+    const int32_t s = A.rowptr[i], e = A.rowptr[i + 1];
+    for (int32_t p = s + lane; p < e; p += 32) {
+      const int32_t k = A.col[p];
+      const int32_t d = t_rowptr[k] + atomicAdd(&cursor[k], 1);
+      tmp_col[d] = (int32_t)i;
+      tmp_val[d] = A.val[p];
+    }
+  }
+}
+
+// ---- segment sort --------------------------------------------------------------
+constexpr int kShortSeg = 256;      // warp + shared bitonic
+constexpr int kMidSeg = 8192;       // CTA + shared bitonic
+constexpr int kLongThreads = 512;
+constexpr int kLongWindow = 1 << 18;  // bitmap bits of the long-segment counting sort
+
+__device__ __forceinline__ int64_t seg_src(const SegSortArgs& a, int64_t s) {
+  return a.src_off64 ? a.src_off64[s] : (int64_t)a.src_off32[s];
+}
+__device__ __forceinline__ int64_t seg_dst(const SegSortArgs& a, int64_t s) {
+  return a.dst_off64 ? a.dst_off64[s] : (int64_t)a.dst_off32[s];
+}
+__device__ __forceinline__ int64_t seg_len(const SegSortArgs& a, int64_t s) {
+  return a.lens ? (int64_t)a.lens[s] : seg_src(a, s + 1) - seg_src(a, s);
+}
+
+__global__ void __launch_bounds__(256) k_segsort_short(SegSortArgs a) {
+  __shared__ int skeys[8][kShortSeg];
+  __shared__ double svals[8][kShortSeg];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const WarpGroup g(32);
+  int* keys = skeys[w];
+  double* vals = svals[w];
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t s = warp; s < a.nseg; s += nwarps) {
+    const int64_t len = seg_len(a, s);
+    if (len <= 0) continue;
+    const int64_t so = seg_src(a, s), dof = seg_dst(a, s);
+    if (len > kShortSeg) {
+      if (lane == 0) a.long_list[atomicAdd(a.long_count, 1)] = (int32_t)s;
+      continue;
+    }
+    const int P = next_pow2_int((int)len);
+    for (int i = lane; i < P; i += 32) {
+      if (i < len) {
+        keys[i] = a.src_key[so + i];
+        vals[i] = a.src_val[so + i];
+      } else {
+        keys[i] = INT_MAX;
+      }
+    }
+    __syncwarp();
+    bitonic_sort_pairs(g, keys, vals, P);
+    for (int i = lane; i < len; i += 32) {
+      a.dst_key[dof + i] = keys[i];
+      a.dst_val[dof + i] = vals[i];
+    }
+    __syncwarp();
+  }
+}
+
+// Long segments (count read on the device): bitonic in shared memory up to
+// kMidSeg entries, else a counting sort over bitmap windows of the key range
+// (keys are unique, so a key's rank is the number of set bits below it).
+__global__ void __launch_bounds__(kLongThreads) k_segsort_long(SegSortArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ long long scratch[33];
+  __shared__ int s_minmax[2];
+  const CtaGroup g;
+  const int nlong = *a.long_count;
+  for (int li = blockIdx.x; li < nlong; li += gridDim.x) {
+    const int64_t s = a.long_list[li];
+    const int64_t len = seg_len(a, s);
+    const int64_t so = seg_src(a, s), dof = seg_dst(a, s);
+    if (len <= kMidSeg) {
+      double* vals = (double*)smem;
+      int* keys = (int*)(vals + kMidSeg);
+      const int P = next_pow2_int((int)len);
+      for (int i = threadIdx.x; i < P; i += blockDim.x) {
+        if (i < len) {
+          keys[i] = a.src_key[so + i];
+          vals[i] = a.src_val[so + i];
+        } else {
+          keys[i] = INT_MAX;
+        }
+      }
+      __syncthreads();
+      bitonic_sort_pairs(g, keys, vals, P);
+      for (int i = threadIdx.x; i < len; i += blockDim.x) {
+        a.dst_key[dof + i] = keys[i];
+        a.dst_val[dof + i] = vals[i];
+      }
+      __syncthreads();
+      continue;
+    }
+    // key range of the segment
+    if (threadIdx.x == 0) {
+      s_minmax[0] = INT_MAX;
+      s_minmax[1] = -1;
+    }
+    __syncthreads();
+    int mn = INT_MAX, mx = -1;
+    for (int64_t i = threadIdx.x; i < len; i += blockDim.x) {
+      const int k = a.src_key[so + i];
+      mn = min(mn, k);
+      mx = max(mx, k);
+    }
+    atomicMin(&s_minmax[0], mn);
+    atomicMax(&s_minmax[1], mx);
+    __syncthreads();
+    const int kmin = s_minmax[0], kmax = s_minmax[1];
+    uint32_t* bm = (uint32_t*)smem;
+    int* pre = (int*)(bm + kLongWindow / 32);
+    int64_t written = 0;
+    for (long long w0 = kmin; w0 <= kmax; w0 += kLongWindow) {
+      const int nwords = (int)min((long long)kLongWindow / 32, (kmax - w0) / 32 + 1);
+      for (int i = threadIdx.x; i < nwords; i += blockDim.x) bm[i] = 0u;
+      __syncthreads();
+      for (int64_t i = threadIdx.x; i < len; i += blockDim.x) {
+        const long long d = (long long)a.src_key[so + i] - w0;
+        if (d >= 0 && d < (long long)nwords * 32) atomicOr(&bm[d >> 5], 1u << (d & 31));
+      }
+      __syncthreads();
+      const int per = (nwords + blockDim.x - 1) / blockDim.x;
+      const int wb = min(nwords, (int)threadIdx.x * per), we = min(nwords, wb + per);
+      int local = 0;
+      for (int i = wb; i < we; ++i) local += __popc(bm[i]);
+      int tot;
+      int run = block_exclusive_scan(local, (int*)scratch, &tot);
+      for (int i = wb; i < we; ++i) {
+        pre[i] = run;
+        run += __popc(bm[i]);
+      }
+      __syncthreads();
+      for (int64_t i = threadIdx.x; i < len; i += blockDim.x) {
+        const int key = a.src_key[so + i];
+        const long long d = (long long)key - w0;
+        if (d >= 0 && d < (long long)nwords * 32) {
+          const int wi = (int)(d >> 5), b = (int)(d & 31);
+          const int64_t pos = written + pre[wi] + __popc(bm[wi] & ((1u << b) - 1u));
+          if (pos < len) {
+            a.dst_key[dof + pos] = key;
+            a.dst_val[dof + pos] = a.src_val[so + i];
+          }
+        }
+      }
+      written += tot;
+      __syncthreads();
+    }
+    if (written != len && threadIdx.x == 0) report(a.status, DEV_ERR_OVERFLOW);
+    __syncthreads();
+  }
+}
+
+static size_t long_smem_bytes() {
+  const size_t bitonic = (size_t)kMidSeg * 12;
+  const size_t bitmap = (size_t)kLongWindow / 32 * 8;
+  return bitonic > bitmap ? bitonic : bitmap;
+}
+
+cudaError_t launch_segsort(const SegSortArgs& a, int num_sms, cudaStream_t s) {
+  if (a.nseg <= 0) return cudaSuccess;
+  cudaError_t e = cudaMemsetAsync(a.long_count, 0, sizeof(int32_t), s);
+  if (e != cudaSuccess) return e;
+  int64_t blocks = ((int64_t)a.nseg * 32 + 255) / 256;
+  const int64_t cap = (int64_t)num_sms * 8;
+  if (blocks > cap) blocks = cap;
+  k_segsort_short<<<(unsigned)blocks, 256, 0, s>>>(a);
+  SPG_COUNT_LAUNCH();
+  const size_t smem = long_smem_bytes();
+  e = cudaFuncSetAttribute(k_segsort_long, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k_segsort_long<<<(unsigned)(num_sms * 2), kLongThreads, smem, s>>>(a);
+  SPG_COUNT_LAUNCH();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_transpose(const MatView& A, int32_t* t_rowptr, int32_t* t_col, double* t_val,
+                             const TransposeWork& w, int num_sms, cudaStream_t s) {
+  const int32_t n = A.n;
+  cudaError_t e = cudaMemsetAsync(w.cnt, 0, sizeof(int32_t) * (size_t)(n > 0 ? n : 1), s);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(w.cursor, 0, sizeof(int32_t) * (size_t)(n > 0 ? n : 1), s);
+  if (e != cudaSuccess) return e;
+  if ((e = launch_col_count(A, w.cnt, s)) != cudaSuccess) return e;
+  if ((e = launch_scan_i32_i32(w.cnt, t_rowptr, n, w.scan_tmp, s)) != cudaSuccess) return e;
+  if (A.nnz == 0 || n == 0) return cudaSuccess;
+  int64_t blocks = ((int64_t)n * 32 + 255) / 256;
+  const int64_t cap = (int64_t)num_sms * 16;
+  if (blocks > cap) blocks = cap;
+  k_transpose_scatter<<<(unsigned)blocks, 256, 0, s>>>(A, t_rowptr, w.cursor, w.tmp_col,
+                                                       w.tmp_val);
+  SPG_COUNT_LAUNCH();
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  SegSortArgs sa{};
+  sa.nseg = n;
+  sa.src_off32 = t_rowptr;
+  sa.dst_off32 = t_rowptr;
+  sa.src_key = w.tmp_col;
+  sa.src_val = w.tmp_val;
+  sa.dst_key = t_col;
+  sa.dst_val = t_val;
+  sa.key_bound = n;
+  sa.long_list = w.long_list;
+  sa.long_count = w.long_count;
+  sa.status = w.status;
+  return launch_segsort(sa, num_sms, s);
+}
+
+}  // namespace spg

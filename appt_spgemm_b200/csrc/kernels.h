@@ -1,0 +1,191 @@
+// Host-side launchers of the engine's kernels (defined in the k_*.cu files).
+// Every launcher is asynchronous on `stream` and returns the launch error.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "device_common.cuh"
+#include "internal.h"
+
+namespace spg {
+
+// Kernels launched by the engine on this thread (every <<<>>> site counts).
+extern thread_local long long g_kernel_launches;
+#define SPG_COUNT_LAUNCH() (++::spg::g_kernel_launches)
+
+// ---- validation / pre-pass / binning (k_prepass.cu) --------------------------
+
+// Flags DEV_ERR_BAD_INDEX / sets *bad (device int) when A is not a square CSR
+// with rowptr[0]=0, monotone rowptr, rowptr[n]=nnz, columns in [0,n) strictly
+// increasing within each row.
+cudaError_t launch_validate(const MatView& A, uint32_t* status, cudaStream_t s);
+
+// Per row i of C = A·B: products f_i = Σ_{k∈A_i} nnz(B_k) and the column span
+// [lo_i, hi_i] of the output row (B rows sorted).  Rows with f_i = 0 get
+// lo = INT_MAX, hi = -1.
+cudaError_t launch_prepass(const MatView& A, const MatView& B, int64_t* f, int32_t* lo,
+                           int32_t* hi, cudaStream_t s);
+
+// What a row's bin is computed from.
+struct BinSource {
+  int mode;                 // 0: symbolic (from products and span), 1: numeric (from counts)
+  int32_t n;
+  const int64_t* f;
+  const int32_t* lo;
+  const int32_t* hi;
+  const int32_t* rownnz;    // numeric: entries of the row (plain) or the row total (gram)
+  const int32_t* rowlow;    // numeric gram: lower-part count (bin uses rownnz − rowlow)
+  int max_log2;             // largest shared table (log2 slots) before the heavy path
+  int force_heavy;
+};
+
+__host__ __device__ __forceinline__ int ceil_log2_64(int64_t x) {
+  int l = 0;
+  while (((int64_t)1 << l) < x) ++l;
+  return l;
+}
+
+// Table size rule: symbolic tables hold keys only and are sized for load ≤ 3/4
+// of min(products, span); numeric tables hold key+value for load ≤ 2/3 of the
+// exact row count.  Bin b in 1..kNumTableBins means 2^(b+kMinTableLog2−1) slots.
+__host__ __device__ __forceinline__ int row_bin(const BinSource& s, int i) {
+  int64_t size;
+  int64_t want;
+  if (s.mode == 0) {
+    int64_t f = s.f[i];
+    if (f <= 0) return kEmptyBin;
+    int64_t span = (int64_t)s.hi[i] - (int64_t)s.lo[i] + 1;
+    size = f < span ? f : span;
+    want = size + size / 3 + 1;
+  } else {
+    int64_t m = s.rownnz[i] - (s.rowlow ? s.rowlow[i] : 0);
+    if (m <= 0) return kEmptyBin;
+    size = m;
+    want = m + m / 2 + 1;
+  }
+  if (s.force_heavy) return kHeavyBin;
+  int lg = ceil_log2_64(want);
+  if (lg < kMinTableLog2) lg = kMinTableLog2;
+  if (lg > s.max_log2) return kHeavyBin;
+  return lg - kMinTableLog2 + 1;
+}
+
+constexpr int kBinRowsPerBlock = 1024;  // rows per block of the binning kernels
+
+// Stable binning: rows of each bin listed in increasing row order.
+//   hist:  int32[kNumBins * nblocks] (bin-major), nblocks = ceil(n / 1024)
+//   counts_out: int64[2*kNumBins] on the device → {count[b]} then {start[b]}
+cudaError_t launch_bin_rows(const BinSource& src, int32_t* hist, int64_t* counts_out,
+                            int32_t* rows_out, cudaStream_t s);
+
+// Exclusive scan of int32 counts into int64 offsets out[0..n], out[n] = total.
+// `tmp` needs scan_tmp_bytes(n) bytes.
+size_t scan_tmp_bytes(int64_t n);
+cudaError_t launch_scan_i32_i64(const int32_t* in, int64_t* out, int64_t n, void* tmp,
+                                cudaStream_t s);
+// Same with int32 output (caller guarantees the total fits in int32).
+cudaError_t launch_scan_i32_i32(const int32_t* in, int32_t* out, int64_t n, void* tmp,
+                                cudaStream_t s);
+
+// ---- shared-memory hash rows (k_rows.cu) ------------------------------------
+
+struct RowArgs {
+  MatView A, B;
+  const int32_t* rows;      // this bin's rows
+  int32_t nrows;
+  int32_t G;                // lanes per row (warp bins); CTA bins use blockDim
+  // symbolic outputs
+  int32_t* rownnz;
+  int32_t* rowlow;          // gram: columns < row
+  // numeric inputs / outputs
+  const int64_t* rowptr;    // C row pointers
+  const int32_t* cnt_in;    // symbolic counts (expected entries)
+  const int32_t* low_in;    // gram: lower counts
+  int32_t* ccol;
+  double* cval;
+  // gram mirror: strict-upper entries appended to a temporary lower store
+  const int64_t* lowptr;
+  int32_t* cursor;
+  int32_t* lcol;
+  double* lval;
+  uint32_t* status;
+};
+
+// Launch the kernel of one table bin (1..kNumTableBins).  `gram` selects the
+// A·Aᵀ upper-triangle variant (symbolic: split lower/upper counts; numeric:
+// upper part only plus the mirror append).
+cudaError_t launch_hash_bin(int bin, bool numeric, bool gram, const RowArgs& a, int num_sms,
+                            cudaStream_t s);
+int hash_bin_lanes(int bin, int lanes_cfg);
+
+// ---- heavy rows: dense column windows (k_heavy.cu) --------------------------
+struct HeavyArgs {
+  RowArgs r;                // rows = heavy list, outputs as in RowArgs
+  const int32_t* lo;        // output column span per row
+  const int32_t* hi;
+  int32_t window_bits;      // W (multiple of 32 * threads)
+};
+cudaError_t launch_heavy(bool numeric, bool gram, const HeavyArgs& a, int threads, int num_sms,
+                         cudaStream_t s);
+size_t heavy_smem_bytes(bool numeric, int threads, int window_bits);
+
+// ---- transpose and segment sort (k_transpose.cu) ----------------------------
+
+// Counting-sort transpose: t_rowptr (n+1) gets the column histogram scan,
+// entries are appended per column with atomic cursors into (tmp_col, tmp_val),
+// then each column is sorted by row into (t_col, t_val).
+// Workspace: cnt/cursor int32[n], scan tmp, tmp_col/tmp_val [nnz], long list.
+struct TransposeWork {
+  int32_t* cnt;
+  int32_t* cursor;
+  void* scan_tmp;
+  int32_t* tmp_col;
+  double* tmp_val;
+  int32_t* long_list;   // int32[n]
+  int32_t* long_count;  // int32[1]
+  uint32_t* status;
+};
+cudaError_t launch_transpose(const MatView& A, int32_t* t_rowptr, int32_t* t_col, double* t_val,
+                             const TransposeWork& w, int num_sms, cudaStream_t s);
+
+// Sort segments of unique int keys (with double payloads) from a source store
+// into a destination store.  Segment s: source [src_off[s], +len), destination
+// [dst_off[s], +len), len = lens ? lens[s] : src_off[s+1] − src_off[s].
+struct SegSortArgs {
+  int32_t nseg;
+  const int64_t* src_off64;
+  const int32_t* src_off32;
+  const int64_t* dst_off64;
+  const int32_t* dst_off32;
+  const int32_t* lens;
+  const int32_t* src_key;
+  const double* src_val;
+  int32_t* dst_key;
+  double* dst_val;
+  int32_t key_bound;     // keys lie in [0, key_bound)
+  int32_t* long_list;
+  int32_t* long_count;
+  uint32_t* status;
+};
+cudaError_t launch_segsort(const SegSortArgs& a, int num_sms, cudaStream_t s);
+
+// ---- descriptors ------------------------------------------------------------
+struct DescAccum {        // device accumulators of spg_describe
+  unsigned long long sum_deg2;   // Σ deg²
+  unsigned long long prod_aa;    // Σ_{(i,k)} deg(k)
+  unsigned long long prod_aat;   // Σ_k colcount²
+  unsigned long long sym_hits;   // entries (i,j) with (j,i) present
+  int max_deg;
+  int max_col_deg;
+  int bandwidth;
+  int pad;
+};
+cudaError_t launch_describe(const MatView& A, const int32_t* colcount, DescAccum* acc,
+                            cudaStream_t s);
+// out[0] = Σ f, out[1] = max f, out[2] = max rownnz (out zeroed by the launcher).
+cudaError_t launch_row_stats(const int64_t* f, const int32_t* rownnz, int32_t n,
+                             unsigned long long* out, cudaStream_t s);
+cudaError_t launch_col_count(const MatView& A, int32_t* cnt, cudaStream_t s);
+
+}  // namespace spg

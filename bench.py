@@ -1,0 +1,471 @@
+#!/usr/bin/env python3
+"""SpGEMM benchmark: GFLOP/s (2 × intermediate products / s) of C = A·A and
+C = A·Aᵀ on one B200, with the roofline of the dominant kernel, the CPU oracle
+timed on the host cores, cuSPARSE on the same GPU, and an end-to-end number
+through the public API with host buffers.
+
+Workload: the 3-D 27-point stencil on a 96³ grid (n = 884,736, nnz = 23.4M,
+values uniform(−1,1) from a seed), structurally symmetric, numerically
+unsymmetric; one step = one A·A plus one A·Aᵀ (the engine's Gram path).
+Inputs (284 MB) and outputs (2 × 1.3 GB) exceed the 126 MB L2, so no flush
+is needed between steps.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Multi-GPU: the product has no exchange step, so N GPUs run N independent
+replicas (weak scaling); the time is the max over ranks.  --impl reference
+times the CPU oracle (the reference's algorithm, restated) on the host cores.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SIDE = 96
+SEED = 2
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+TRAFFIC = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawTextHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--side", type=int, default=SIDE, help="stencil grid side (96 = the benchmark)")
+    ap.add_argument("--aat-task", default="AAtS", choices=["AAt", "AAtS"],
+                    help="engine task used for A·Aᵀ")
+    ap.add_argument("--no-baselines", action="store_true",
+                    help="skip the CPU oracle, cuSPARSE and reference-GPU baselines")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0,
+                    help="CPU work of the oracle baseline sample")
+    return ap.parse_args()
+
+
+def workload(side):
+    from appt_spgemm_b200 import csr
+    A = csr.stencil27(side, seed=SEED)
+    return A, csr.products(A, "AA"), csr.products(A, "AAt")
+
+
+def config(args, A, extra=None):
+    c = {"workload": f"27-point stencil {args.side}^3 (n={A.n}, nnz={A.nnz}), FP64, "
+                     f"one step = A·A + A·Aᵀ",
+         "matrix": "stencil27", "grid_side": args.side, "n": A.n, "nnz": A.nnz,
+         "tasks": ["AA", "AAt"], "index": "int32 in / int64 C rowptr", "values": "fp64",
+         "l2": "inputs (284 MB) and outputs (2.6 GB) exceed L2; no flush needed",
+         "parallelism": f"replicas x{args.gpus}"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def hbm_peak():
+    try:
+        with open(MEASURED_PEAKS) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        try:
+            rows = [ln.split(",") for ln in open(self.path).read().strip().splitlines()]
+        except Exception:
+            return out
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, r[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        if sm:
+            out.update(sm_mhz=statistics.median(sm), sm_max_mhz=max(mx),
+                       reasons=sorted(reasons), samples=len(sm))
+        try:
+            os.unlink(self.path)
+        except Exception:
+            pass
+        return out
+
+
+# ---------------------------------------------------------------------------
+# CPU baselines (the oracle: test infrastructure, timed here as the baseline)
+# ---------------------------------------------------------------------------
+def row_products(A, B):
+    import numpy as np
+    deg_b = np.diff(B.rowptr).astype(np.int64)
+    per_entry = deg_b[A.col]
+    cs = np.concatenate([[0], np.cumsum(per_entry)])
+    return cs[A.rowptr[1:]] - cs[A.rowptr[:-1]]
+
+
+def cpu_oracle_rate(A, seconds, nthreads, label_rows=None):
+    """Time the oracle on leading row blocks of A·A and A·Aᵀ for about
+    `seconds`; returns (GFLOP/s, products timed, description)."""
+    import numpy as np
+
+    import oracle
+    B_t = A.transpose()
+    total_products = 0
+    total_time = 0.0
+    parts = []
+    for task, B in (("AA", A), ("AAt", B_t)):
+        f = row_products(A, B)
+        budget = seconds / 2
+        r0, r = 0, 256
+        while r0 < A.n and budget > 0:
+            r1 = min(A.n, r0 + r)
+            t0 = time.perf_counter()
+            oracle.rows_stream(A, B, r0, r1, nthreads)
+            dt = time.perf_counter() - t0
+            total_time += dt
+            total_products += int(f[r0:r1].sum())
+            budget -= dt
+            rate = (r1 - r0) / max(dt, 1e-6)
+            r0 = r1
+            r = int(max(256, min(rate * min(budget, 2.0), A.n)))
+        parts.append(f"{task}: rows [0, {r0}) of {A.n}")
+    gflops = 2.0 * total_products / total_time / 1e9
+    return gflops, total_products, total_time, "; ".join(parts)
+
+
+def run_reference(args):
+    """--impl reference: the reference's algorithm on the host cores (the CPU
+    oracle restating it, all threads), same workload, metric and config; each
+    step is a bounded sample of rows of both products."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle
+    A, p_aa, p_aat = workload(args.side)
+    nthreads = os.cpu_count() or 1
+    B_t = A.transpose()
+    f_aa, f_aat = row_products(A, A), row_products(A, B_t)
+    # size one step to about 4 s of work: calibrate on a small block
+    t0 = time.perf_counter()
+    oracle.rows_stream(A, A, 0, 512, nthreads)
+    rate_rows = 512 / max(time.perf_counter() - t0, 1e-6)
+    rows = int(min(A.n, max(512, rate_rows * 2.0)))
+    times, prods = [], []
+    for step in range(args.warmup + args.steps):
+        r0 = (step * rows) % max(1, A.n - rows + 1)
+        t0 = time.perf_counter()
+        oracle.rows_stream(A, A, r0, r0 + rows, nthreads)
+        oracle.rows_stream(A, B_t, r0, r0 + rows, nthreads)
+        dt = time.perf_counter() - t0
+        if step >= args.warmup:
+            times.append(dt)
+            prods.append(int(f_aa[r0:r0 + rows].sum() + f_aat[r0:r0 + rows].sum()))
+    gflops = 2.0 * sum(prods) / sum(times) / 1e9
+    sample = (f"{rows} consecutive rows of A·A and of A·Aᵀ per step "
+              f"({100.0 * rows / A.n:.2f}% of the rows)")
+    line = {"metric": "GFLOP/s (2×intermediate products/s) A·A & A·Aᵀ", "value": round(gflops, 3),
+            "unit": "GFLOP/s", "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(1e3 * statistics.mean(times), 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator)",
+            "config": config(args, A, {"device": "host CPU"}),
+            "cpu_baseline": {"value": round(gflops, 3), "unit": "GFLOP/s", "cores": nthreads,
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": round(gflops, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU baselines outside the timed region: cuSPARSE, the reference's CUDA engine
+# ---------------------------------------------------------------------------
+def cusparse_baseline(dA, A, p_aa, p_aat):
+    import ctypes
+
+    from appt_spgemm_b200 import _capi
+    try:
+        L = ctypes.CDLL(_capi.CUSPARSE_LIB_PATH)
+    except OSError as e:
+        return {"error": str(e)}
+    fn = L.spgb_cusparse_time
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                   ctypes.c_longlong, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_float),
+                   ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_longlong),
+                   ctypes.POINTER(ctypes.c_double), ctypes.c_char_p, ctypes.c_int]
+    out = {}
+    for task, tid, prods in (("AA", 0, p_aa), ("AAt", 1, p_aat)):
+        mean, mn = ctypes.c_float(), ctypes.c_float()
+        nnz = ctypes.c_longlong()
+        chk = (ctypes.c_double * 3)()
+        err = ctypes.create_string_buffer(256)
+        rc = fn(tid, dA.rowptr.data_ptr(), dA.col.data_ptr(), dA.val.data_ptr(), A.n, A.nnz, 5, 2,
+                ctypes.byref(mean), ctypes.byref(mn), ctypes.byref(nnz), chk, err, 256)
+        if rc != 0:
+            out[task] = {"error": err.value.decode()}
+        else:
+            out[task] = {"ms_mean": round(mean.value, 4), "ms_min": round(mn.value, 4),
+                         "nnz_c": nnz.value,
+                         "gflops": round(2.0 * prods / (mean.value * 1e-3) / 1e9, 3)}
+    return out
+
+
+def reference_gpu_baseline(A, p_aa, p_aat):
+    """The reference's own CUDA engine (src/spgemm.cu built unmodified for sm_80,
+    JIT-run on the B200) on a CSR1 file of the same matrix, reps=5."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "spgemm_ref")
+    if not os.path.exists(exe):
+        return {"error": "reference engine binary not built"}
+    from appt_spgemm_b200 import csr
+    out = {}
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "a.csr")
+        csr.write_bin(A, path)
+        for task, prods in (("AA", p_aa), ("AAt", p_aat), ("AAtS", p_aat)):
+            try:
+                r = subprocess.run([exe, "bench", path, task, "5"], capture_output=True, text=True,
+                                   timeout=300)
+                res = [ln.split(",") for ln in r.stdout.splitlines() if ln.startswith("RESULT,")]
+                if r.returncode != 0 or not res:
+                    out[task] = {"error": (r.stderr or r.stdout).strip()[-200:]}
+                    continue
+                ms = float(res[0][6])
+                out[task] = {"ms_mean": ms, "nnz_c": int(res[0][5]),
+                             "gflops": round(2.0 * prods / (ms * 1e-3) / 1e9, 3)}
+            except subprocess.TimeoutExpired:
+                out[task] = {"error": "timeout"}
+    return out
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+
+    from appt_spgemm_b200.engine import CsrDevice, Engine
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+
+    A, p_aa, p_aat = workload(args.side)
+    work_per_step = 2.0 * (p_aa + p_aat)
+    dA = CsrDevice.from_host(A, dev)
+    eng = Engine(dev)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        C1 = eng.multiply(dA, "AA")
+        C2 = eng.multiply(dA, args.aat_task)
+        return C1, C2
+
+    for _ in range(max(args.warmup, 0)):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+    eng.profile_reset()
+    eng.profile_enable(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        e0.record(stream)
+        for _ in range(args.steps):
+            C = step()
+            del C
+        e1.record(stream)
+        torch.cuda.synchronize()
+    eng.profile_enable(False)
+    prof = eng.profile_read()
+    ms = e0.elapsed_time(e1) / max(args.steps, 1)
+    if world > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    value = world * work_per_step / (ms * 1e-3) / 1e9
+
+    # per-task info, dominant kernel and its roofline
+    infos = {}
+    for task in ("AA", args.aat_task):
+        p = eng.plan(dA, task)
+        infos[task] = dict(p.info)
+        p.close()
+    kernels = prof.get("kernels", {})
+    top = max(kernels.items(), key=lambda kv: kv[1]["ms"]) if kernels else None
+    peak, peak_kind = hbm_peak()
+    n, nnz = A.n, A.nnz
+    roofline = None
+    if top:
+        label, rec = top
+        per_launch_ms = rec["ms"] / max(rec["count"], 1)
+        # algorithmic bytes per launch (per call of the phase): numeric kernels
+        # read A once and write C once; symbolic kernels read A's structure and
+        # write one count per row; the transpose reads and writes A once.
+        nnz_c_mean = statistics.mean(i["nnz_c"] for i in infos.values())
+        if label.startswith("num/"):
+            alg = 4 * (n + 1) + 12 * nnz + 8 * (n + 1) + 12 * nnz_c_mean
+        elif label.startswith("sym/"):
+            alg = 4 * (n + 1) + 4 * nnz + 4 * n
+        elif label == "plan/transpose":
+            alg = 2 * (4 * (n + 1) + 12 * nnz)
+        else:
+            alg = 4 * (n + 1) + 12 * nnz
+        achieved = alg / (per_launch_ms * 1e-3) / 1e9
+        traffic = None
+        try:
+            with open(TRAFFIC) as f:
+                traffic = json.load(f).get(label)
+        except Exception:
+            pass
+        roofline = {"bound": "hbm", "kernel": label, "achieved": round(achieved, 1),
+                    "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                    "peak_source": peak_kind, "traffic": traffic,
+                    "alg_bytes_per_launch": int(alg), "ms_per_launch": round(per_launch_ms, 4),
+                    "share_of_step": round(rec["ms"] / (ms * args.steps), 4)}
+    call_alg = sum(4 * (n + 1) + 12 * nnz + 8 * (n + 1) + 12 * i["nnz_c"] for i in infos.values())
+
+    result = {"metric": "GFLOP/s (2×intermediate products/s) A·A & A·Aᵀ",
+              "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world,
+              "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
+              "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+              "data": "synthetic (seeded generator)",
+              "config": config(args, A, {"aat_task": args.aat_task}),
+              "roofline": roofline,
+              "call_roofline": {"alg_bytes_per_step": int(call_alg),
+                                "achieved": round(call_alg / (ms * 1e-3) / 1e9, 1),
+                                "frac": round(call_alg / (ms * 1e-3) / 1e9 / peak, 4),
+                                "unit": "GB/s"},
+              "gpu_launches": int(prof.get("launches", 0)),
+              "kernels_ms_per_step": {k: round(v["ms"] / args.steps, 4)
+                                      for k, v in sorted(kernels.items())},
+              "products": {"AA": p_aa, "AAt": p_aat},
+              "nnz_c": {t: i["nnz_c"] for t, i in infos.items()},
+              "clocks": clocks.summary()}
+
+    # end to end through the public API: host CSR in pinned memory → device,
+    # both products, C back to pinned host buffers, every step
+    if rank == 0 or world > 1:
+        pin = lambda x: torch.from_numpy(x).pin_memory()  # noqa: E731
+        h_rp, h_col, h_val = pin(A.rowptr), pin(A.col), pin(A.val)
+        d_rp = torch.empty_like(dA.rowptr)
+        d_col = torch.empty_like(dA.col)
+        d_val = torch.empty_like(dA.val)
+        outs = {t: (torch.empty(n + 1, dtype=torch.int64).pin_memory(),
+                    torch.empty(infos[t]["nnz_c"], dtype=torch.int32).pin_memory(),
+                    torch.empty(infos[t]["nnz_c"], dtype=torch.float64).pin_memory())
+                for t in infos}
+        h2d = h_rp.numel() * 4 + h_col.numel() * 4 + h_val.numel() * 8
+        d2h = sum((n + 1) * 8 + infos[t]["nnz_c"] * 12 for t in infos)
+
+        def e2e_step():
+            d_rp.copy_(h_rp, non_blocking=True)
+            d_col.copy_(h_col, non_blocking=True)
+            d_val.copy_(h_val, non_blocking=True)
+            M = CsrDevice(n, d_rp, d_col, d_val)
+            for t in ("AA", args.aat_task):
+                C = eng.multiply(M, t)
+                o = outs[t]
+                o[0].copy_(C.rowptr, non_blocking=True)
+                o[1].copy_(C.col, non_blocking=True)
+                o[2].copy_(C.val, non_blocking=True)
+
+        e2e_steps = max(1, min(args.steps, 5))
+        e2e_step()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(e2e_steps):
+            e2e_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = e0.elapsed_time(e1) / e2e_steps
+        result["e2e"] = {"value": round(work_per_step / (e2e_ms * 1e-3) / 1e9, 3),
+                         "unit": "GFLOP/s", "h2d_bytes_per_step": int(h2d),
+                         "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_ms, 3),
+                         "api": "Engine.multiply (spg_plan_create + spg_execute)"}
+
+    if rank == 0 and world == 1 and not args.no_baselines:
+        nthreads = os.cpu_count() or 1
+        gf, prods, secs, sample = cpu_oracle_rate(A, args.cpu_seconds, nthreads)
+        result["cpu_baseline"] = {"value": round(gf, 3), "unit": "GFLOP/s", "cores": nthreads,
+                                  "kind": "port", "sample": sample + f" ({prods} products, "
+                                  f"{secs:.1f} s)"}
+        result["baselines"] = {"cusparse": cusparse_baseline(dA, A, p_aa, p_aat),
+                               "reference_gpu_engine": reference_gpu_baseline(A, p_aa, p_aat)}
+        cs = result["baselines"]["cusparse"]
+        if all("ms_mean" in cs.get(t, {}) for t in ("AA", "AAt")):
+            cms = cs["AA"]["ms_mean"] + cs["AAt"]["ms_mean"]
+            result["baselines"]["cusparse_step_gflops"] = round(work_per_step / (cms * 1e-3) / 1e9, 3)
+
+    eng.close()
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,253 @@
+/*
+ * spgemm_b200.h — C ABI of the B200 (sm_100a) FP64 SpGEMM engine.
+ *
+ * Computes C = A·A, C = A·Aᵀ (plain) and C = A·Aᵀ through the symmetric Gram
+ * path (upper triangle computed, lower triangle mirrored) for a square n×n CSR
+ * matrix A with int32 row pointers / column indices and FP64 values, on one GPU.
+ *
+ * The reference surface this replaces is the header-only engine
+ *   static EngResult run_ours(const char* task, const int* dOff, const int* dCol,
+ *                             const double* dVal, int n, int64_t nnz, int reps);
+ * (src/spgemm_engine.cuh:132-133), its result record EngResult
+ * (src/spgemm_engine.cuh:129) and the CSR1 loader load_bin
+ * (src/spgemm_engine.cuh:21-32).  spg_run_ours() reproduces run_ours; the
+ * spg_plan_* / spg_execute / spg_multiply calls expose what run_ours keeps
+ * internal (the product C itself, with int64 row pointers).
+ *
+ * Conventions
+ *  - Every call returns an spg_status; nothing prints or exits.  The text of the
+ *    last error on the calling thread is spg_last_error_string().
+ *  - Device pointers are borrowed; streams are cudaStream_t passed as void*.
+ *  - Output semantics are structural (pattern product): entries whose products
+ *    cancel to 0.0 are kept as explicit zeros, as cuSPARSE and the reference do.
+ *  - Column indices of every output row are sorted ascending.  Each output value
+ *    is the sum of its products a_ik·b_kj taken in increasing position of k in
+ *    row i of A, each product rounded before the add (no fused multiply-add), so
+ *    results are bit-reproducible run to run.
+ *  - One context per host thread; calls on one context are stream-ordered.
+ */
+#ifndef SPGEMM_B200_H
+#define SPGEMM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPG_ABI_VERSION 1
+
+typedef enum spg_status {
+  SPG_OK = 0,
+  SPG_ERR_INVALID_ARG = 1,   /* null pointer, bad task, n < 0, ...                */
+  SPG_ERR_INVALID_CSR = 2,   /* rowptr not monotone, column out of range,
+                                unsorted or duplicate columns in a row          */
+  SPG_ERR_OOM = 3,           /* device (or pinned host) allocation failed         */
+  SPG_ERR_CUDA = 4,          /* any other CUDA runtime error                      */
+  SPG_ERR_HASH_FULL = 5,     /* a bounded hash probe ran out (device status word) */
+  SPG_ERR_TIMEOUT = 6,       /* a bounded wait gave up                            */
+  SPG_ERR_UNSUPPORTED = 7,   /* size beyond a documented limit                    */
+  SPG_ERR_BUDGET = 8,        /* request exceeds the memory budget (admission)     */
+  SPG_ERR_NOT_READY = 9,     /* asynchronous result not complete yet              */
+  SPG_ERR_IO = 10            /* CSR1 file could not be read / written             */
+} spg_status;
+
+typedef enum spg_task {
+  SPG_TASK_AA = 0,    /* C = A·A                                        ("AA")   */
+  SPG_TASK_AAT = 1,   /* C = A·Aᵀ, Aᵀ built by the engine's transpose   ("AAt")  */
+  SPG_TASK_AATS = 2   /* C = A·Aᵀ via upper triangle + mirror           ("AAtS") */
+} spg_task;
+
+/* Square CSR matrix on the device, borrowed (int32 row pointers: nnz < 2^31). */
+typedef struct spg_csr_dev {
+  int32_t n;
+  int64_t nnz;
+  const int32_t* rowptr; /* n+1 */
+  const int32_t* col;    /* nnz, sorted and unique within each row */
+  const double* val;     /* nnz */
+} spg_csr_dev;
+
+/* Output CSR with int64 row pointers.  For spg_execute the caller owns the
+ * buffers (rowptr: n+1, col/val: nnz from the plan); for spg_multiply the
+ * engine allocates them from the context pool (release with spg_free). */
+typedef struct spg_csr_out {
+  int32_t n;
+  int64_t nnz;
+  int64_t* rowptr;
+  int32_t* col;
+  double* val;
+} spg_csr_out;
+
+/* Engine tuning.  Zero-initialise and set struct_size = sizeof(spg_config);
+ * every field left 0 takes its default.  The autotuner fills one of these. */
+typedef struct spg_config {
+  int32_t struct_size;
+  int32_t device;             /* CUDA ordinal; 0 → current device (default)     */
+  int32_t lanes_per_row;      /* lanes per row in the sub-warp bins: 4/8/16/32;
+                                 0 → chosen from the mean row length of B        */
+  int32_t max_smem_slots;     /* largest shared-memory numeric table (slots);
+                                 rows beyond go to the heavy path; 0 → 8192      */
+  int32_t heavy_threads;      /* threads per CTA on the heavy path; 0 → 512      */
+  int32_t window_bits;        /* column-window width of the dense heavy path
+                                 (bits of the shared bitmap); 0 → 262144         */
+  int32_t force_heavy;        /* 1 → send every non-empty row to the heavy path
+                                 (debug oracle of the binning, as the reference
+                                 did by forcing its global path)                 */
+  int32_t reserved0;
+  int64_t pool_release_bytes; /* memory-pool release threshold; 0 → keep all    */
+  int64_t reserved[6];
+} spg_config;
+
+/* Result record of spg_run_ours: the reference's EngResult {ms, nnz, s, as, sq}
+ * (src/spgemm_engine.cuh:129) — mean ms per call over `reps`, nnz(C), and the
+ * order-independent checksums Σv, Σ|v|, Σv² of C's values. */
+typedef struct spg_eng_result {
+  float ms;
+  int64_t nnz;
+  double s, as, sq;
+} spg_eng_result;
+
+/* Structural facts gathered by the pre-pass and the symbolic phase. */
+typedef struct spg_plan_info {
+  int32_t n;
+  int32_t task;
+  int64_t nnz_a;
+  int64_t nnz_c;              /* exact, structural                              */
+  int64_t products;           /* Σ_{(i,k)} nnz(B_k): A·A  Σ_k nnz(A_k)… (metric) */
+  int64_t products_computed;  /* products actually multiplied (AAtS: ~half)     */
+  int64_t max_row_products;
+  int64_t max_row_nnz;
+  int64_t heavy_rows;         /* rows on the heavy (CTA-per-row) path           */
+  int64_t workspace_bytes;    /* device workspace held by the plan              */
+  int64_t output_bytes;       /* 8(n+1) + 12·nnz_c                              */
+  int32_t bins_used;
+  int32_t reserved;
+} spg_plan_info;
+
+/* Structural descriptors of A (the reference's dispatcher features,
+ * bench/dispatch.cu:26-38, computed on the device). */
+typedef struct spg_descriptors {
+  int32_t n;
+  int64_t nnz;
+  double mean_deg;
+  double deg_cv;              /* std(row nnz) / mean(row nnz)                    */
+  double fill_aa;             /* Σ_{(i,k)} deg(k) / nnz                          */
+  double fill_aat;            /* Σ_k colcount(k)² / nnz                          */
+  int64_t products_aa;
+  int64_t products_aat;
+  int32_t max_deg;
+  int32_t max_col_deg;
+  int32_t bandwidth;          /* max |i − j| over entries                        */
+  int32_t reserved;
+  double pattern_symmetry;    /* fraction of entries (i,j) with (j,i) present    */
+} spg_descriptors;
+
+typedef struct spg_ctx spg_ctx;
+typedef struct spg_plan spg_plan;
+
+/* ---- version / errors ---------------------------------------------------- */
+int32_t spg_abi_version(void);
+const char* spg_last_error_string(void);
+const char* spg_status_string(spg_status s);
+
+/* ---- context -------------------------------------------------------------- */
+spg_status spg_create(spg_ctx** ctx, const spg_config* cfg);
+spg_status spg_destroy(spg_ctx* ctx);
+/* Device status word written by kernels (bounded probes, …); reading it
+ * synchronises the given stream.  Cleared on read. */
+spg_status spg_check_device_status(spg_ctx* ctx, void* stream);
+
+/* ---- plan / execute (replaces the sizing half of run_ours) ---------------- */
+/* Pre-pass + binning + symbolic phase.  One pinned readback (nnz(C)) is the
+ * only host synchronisation.  A must stay valid until the plan is destroyed. */
+spg_status spg_plan_create(spg_ctx* ctx, spg_task task, const spg_csr_dev* A,
+                           void* stream, spg_plan** plan);
+spg_status spg_plan_get_info(const spg_plan* plan, spg_plan_info* info);
+/* Numeric phase + in-row sort (+ mirror for AAtS) into caller-owned buffers:
+ * C->rowptr (n+1), C->col / C->val (info.nnz_c).  Asynchronous on `stream`. */
+spg_status spg_execute(spg_plan* plan, spg_csr_out* C, void* stream);
+spg_status spg_plan_destroy(spg_plan* plan);
+
+/* plan + execute with C allocated from the context pool; C->nnz is set. */
+spg_status spg_multiply(spg_ctx* ctx, spg_task task, const spg_csr_dev* A,
+                        spg_csr_out* C, void* stream);
+/* Release a buffer returned by spg_multiply (stream-ordered). */
+spg_status spg_free(spg_ctx* ctx, void* dev_ptr, void* stream);
+
+/* ---- profiling ------------------------------------------------------------ */
+/* Per-kernel CUDA events recorded on the launching stream (off by default) and
+ * a count of the engine's kernel launches on the calling thread.
+ * spg_profile_read synchronises the device and writes JSON text
+ *   {"launches": L, "kernels": {"<phase>/<kernel>": {"count": c, "ms": t}, ...}}
+ * covering the calls since the last spg_profile_reset. */
+spg_status spg_profile_enable(spg_ctx* ctx, int32_t enable);
+spg_status spg_profile_reset(spg_ctx* ctx);
+spg_status spg_profile_read(spg_ctx* ctx, char* json, size_t capacity);
+
+/* ---- transpose (CSR → CSR of Aᵀ, counting sort; rows sorted) ------------- */
+/* Replaces k_colcount/k_scatter/build_At (src/spgemm_engine.cuh:37-44,140-146)
+ * with a deterministic result.  Caller-owned outputs: rowptr n+1, col/val nnz. */
+spg_status spg_transpose(spg_ctx* ctx, const spg_csr_dev* A, int32_t* t_rowptr,
+                         int32_t* t_col, double* t_val, void* stream);
+
+/* ---- descriptors ----------------------------------------------------------- */
+spg_status spg_describe(spg_ctx* ctx, const spg_csr_dev* A, spg_descriptors* d,
+                        void* stream);
+
+/* ---- reference-compatible call -------------------------------------------- */
+/* Same semantics as run_ours (src/spgemm_engine.cuh:132-210): task "AA", "AAt"
+ * or "AAtS"; one checked call, then `reps` timed full calls (plan + execute +
+ * transpose), mean ms; nnz(C) and checksums of C's values.  Uses an internal
+ * context on the current device and the legacy default stream. */
+spg_status spg_run_ours(const char* task, const int32_t* dOff, const int32_t* dCol,
+                        const double* dVal, int32_t n, int64_t nnz, int32_t reps,
+                        spg_eng_result* out);
+
+/* Order-independent checksums of a device FP64 array (Σv, Σ|v|, Σv²), summed
+ * on the host in index order like checksum() (src/spgemm_engine.cuh:116-118). */
+spg_status spg_checksum(const double* dev_val, int64_t count, double* s,
+                        double* as, double* sq);
+
+/* ---- CSR1 files (src/export_bin.py:6-8 format, load_bin :21-32) ----------- */
+/* Host CSR in malloc'd buffers; release with spg_host_csr_free. */
+typedef struct spg_host_csr {
+  int32_t n;
+  int64_t nnz;
+  int32_t* rowptr;
+  int32_t* col;
+  double* val;
+} spg_host_csr;
+spg_status spg_csr1_read(const char* path, spg_host_csr* out);
+spg_status spg_csr1_write(const char* path, const spg_host_csr* A);
+void spg_host_csr_free(spg_host_csr* A);
+/* Validate a host CSR (monotone rowptr, columns in range, sorted, unique). */
+spg_status spg_host_csr_validate(const spg_host_csr* A);
+
+/* ---- synthetic generators (host, deterministic, seeded) ------------------- */
+/* 2-D 5-point Laplacian on a side×side grid: 4.0 diagonal, −1.0 neighbours. */
+spg_status spg_gen_laplace2d(int32_t side, spg_host_csr* out);
+/* 3-D 27-point stencil on side³, values uniform(−1,1) from mt19937_64(seed)
+ * drawn per entry in CSR order. */
+spg_status spg_gen_stencil27(int32_t side, uint64_t seed, spg_host_csr* out);
+/* R-MAT: 2^scale rows, edge_factor·2^scale edge draws with quadrant
+ * probabilities (a,b,c,1−a−b−c), duplicates merged into one entry, self-loops
+ * kept, values uniform(0,1) drawn per merged entry in CSR order. */
+spg_status spg_gen_rmat(int32_t scale, int32_t edge_factor, double a, double b,
+                        double c, uint64_t seed, spg_host_csr* out);
+/* Random banded: half-bandwidth bw, each off-diagonal in-band entry kept with
+ * probability fill, diagonal always present, values uniform(−1,1). */
+spg_status spg_gen_banded(int32_t n, int32_t bw, double fill, uint64_t seed,
+                          spg_host_csr* out);
+/* Erdős–Rényi: row nnz ~ Poisson(lambda) (capped at n), columns uniform
+ * without replacement, values uniform(−1,1). */
+spg_status spg_gen_er(int32_t n, double lambda, uint64_t seed, spg_host_csr* out);
+/* Uniform random sparse matrix with exactly `per_row` sorted random columns in
+ * each row (capped at n), values uniform(−1,1); a test workhorse. */
+spg_status spg_gen_uniform(int32_t n, int32_t per_row, uint64_t seed,
+                           spg_host_csr* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPGEMM_B200_H */

@@ -1,0 +1,272 @@
+"""GPU parity: the engine, called through the C ABI, against the CPU oracle.
+
+The bar is bit-exact everywhere: row pointers, sorted column indices and every
+FP64 value (the engine and the oracle both add the rounded products of each
+entry in increasing position of k in row i of A).  The 1e-12 relative bound
+of the task is therefore met with zero error.
+"""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle
+from appt_spgemm_b200 import _capi, csr
+from appt_spgemm_b200._capi import SpgemmError
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+TASKS = ("AA", "AAt", "AAtS")
+
+
+@pytest.fixture(scope="module")
+def eng():
+    from appt_spgemm_b200.engine import Engine
+    e = Engine("cuda:0")
+    yield e
+    e.check_device_status()
+    e.close()
+
+
+def dev(A):
+    from appt_spgemm_b200.engine import CsrDevice
+    return CsrDevice.from_host(A, "cuda:0")
+
+
+def assert_same(C, ref, label):
+    rp, ci, cx = C.to_host()
+    orp, oci, ocx = ref
+    assert rp.shape == orp.shape, label
+    assert np.array_equal(rp, orp), f"{label}: rowptr"
+    assert np.array_equal(ci, oci), f"{label}: col"
+    assert np.array_equal(cx.view(np.int64), ocx.view(np.int64)), (
+        f"{label}: values, max |diff| {np.abs(cx - ocx).max() if len(cx) else 0}")
+
+
+def run_case(eng, A, task, label):
+    C = eng.multiply(dev(A), task)
+    torch.cuda.synchronize()
+    assert_same(C, oracle.multiply(A, task), f"{label}/{task}")
+
+
+@pytest.mark.parametrize("task", TASKS)
+def test_golden_cases(eng, golden, golden_dir, task):
+    for name in golden["cases"]:
+        A = csr.load_bin(os.path.join(golden_dir, name + ".csr"))
+        run_case(eng, A, task, name)
+
+
+@pytest.mark.parametrize("task", TASKS)
+def test_laplacian_64(eng, task):
+    run_case(eng, csr.laplace2d(64), task, "laplace2d_64")
+
+
+# per-row widths that put rows in every shared-table bin and on the heavy path
+@pytest.mark.parametrize("per_row", [1, 2, 3, 5, 8, 12, 16, 24, 32, 48, 64, 96, 128])
+@pytest.mark.parametrize("task", TASKS)
+def test_every_bin(eng, per_row, task):
+    n = 2500 if per_row <= 64 else 4000
+    run_case(eng, csr.uniform(n, per_row, seed=per_row), task, f"uniform{per_row}")
+
+
+@pytest.mark.parametrize("lanes", [4, 8, 16, 32])
+def test_lanes_per_row(lanes):
+    from appt_spgemm_b200.engine import Engine
+    with Engine("cuda:0", lanes_per_row=lanes) as e:
+        for task in TASKS:
+            run_case(e, csr.erdos_renyi(3000, 9.0, seed=lanes), task, f"er/lanes{lanes}")
+
+
+@pytest.mark.parametrize("window", [0, 4096])
+def test_force_heavy_dense_windows(window):
+    """Every row through the CTA-per-row dense-window path (the reference's
+    debugging trick of forcing all rows onto its global path), with one window
+    and with many windows per row."""
+    from appt_spgemm_b200.engine import Engine
+    with Engine("cuda:0", force_heavy=1, window_bits=window) as e:
+        for A, lab in ((csr.laplace2d(40), "lap40"), (csr.rmat(11, 8, seed=2), "rmat11"),
+                       (csr.erdos_renyi(20000, 4.0, seed=3), "er20k")):
+            for task in TASKS:
+                run_case(e, A, task, f"forced/{lab}/w{window}")
+
+
+@pytest.mark.parametrize("task", TASKS)
+def test_rmat_heavy_rows(eng, task):
+    run_case(eng, csr.rmat(13, 16, seed=3), task, "rmat13")
+
+
+@pytest.mark.parametrize("task", TASKS)
+def test_stencil27_small(eng, task):
+    run_case(eng, csr.stencil27(18, seed=2), task, "stencil27_18")
+
+
+@pytest.mark.parametrize("task", TASKS)
+def test_banded_and_er(eng, task):
+    run_case(eng, csr.banded(5000, 40, 0.3, seed=4), task, "banded")
+    run_case(eng, csr.erdos_renyi(6000, 20.0, seed=5), task, "er")
+
+
+def test_edge_shapes(eng):
+    cases = [
+        csr.CsrHost(0, np.zeros(1, np.int32), np.zeros(0, np.int32), np.zeros(0)),
+        csr.CsrHost(1, np.array([0, 1], np.int32), np.array([0], np.int32), np.array([-2.5])),
+        csr.CsrHost(1, np.array([0, 0], np.int32), np.zeros(0, np.int32), np.zeros(0)),
+        csr.CsrHost(7, np.zeros(8, np.int32), np.zeros(0, np.int32), np.zeros(0)),
+    ]
+    n = 3000  # one dense row, one dense column, everything else empty
+    rp = np.zeros(n + 1, np.int32)
+    cols = []
+    for i in range(n):
+        c = list(range(n)) if i == 17 else ([17] if i % 3 == 0 else [])
+        cols.extend(c)
+        rp[i + 1] = len(cols)
+    cases.append(csr.CsrHost(n, rp, np.array(cols, np.int32),
+                             np.linspace(-1, 1, len(cols))))
+    for k, A in enumerate(cases):
+        for task in TASKS:
+            run_case(eng, A, task, f"edge{k}")
+
+
+def test_exact_cancellation_kept(eng):
+    """Structural semantics: products that cancel to 0.0 stay as explicit
+    entries (report/CORRECTNESS_NOTES.md:3-16)."""
+    A = csr.CsrHost(2, np.array([0, 2, 4], np.int32), np.array([0, 1, 0, 1], np.int32),
+                    np.array([1.0, 1.0, 1.0, -1.0]))
+    C = eng.multiply(dev(A), "AA")
+    rp, ci, cx = C.to_host()
+    assert list(rp) == [0, 2, 4] and list(ci) == [0, 1, 0, 1]
+    assert list(cx) == [2.0, 0.0, 0.0, 2.0]
+
+
+def test_invalid_csr_rejected_on_device(eng):
+    from appt_spgemm_b200.engine import CsrDevice
+    A = csr.laplace2d(8)
+    bad = [A.col.copy(), A.col.copy(), A.col.copy()]
+    bad[0][[1, 2]] = bad[0][[2, 1]]          # unsorted row
+    bad[1][2] = bad[1][1]                    # duplicate column
+    bad[2][-1] = 64                          # out of range
+    for c in bad:
+        M = CsrDevice(A.n, torch.from_numpy(A.rowptr).cuda(), torch.from_numpy(c).cuda(),
+                      torch.from_numpy(A.val).cuda())
+        for task in TASKS:
+            with pytest.raises(SpgemmError) as e:
+                eng.multiply(M, task)
+            assert e.value.status == _capi.SPG_ERR_INVALID_CSR
+    with pytest.raises(SpgemmError):
+        eng.multiply(dev(A), "AB")
+
+
+def test_transpose_matches_oracle(eng):
+    for A in (csr.rmat(12, 16, seed=8), csr.laplace2d(30), csr.uniform(1000, 40, seed=2)):
+        T = eng.transpose(dev(A))
+        torch.cuda.synchronize()
+        O = oracle.transpose(A)
+        assert np.array_equal(T.rowptr.cpu().numpy(), O.rowptr)
+        assert np.array_equal(T.col.cpu().numpy(), O.col)
+        assert np.array_equal(T.val.cpu().numpy(), O.val)
+
+
+def test_descriptors(eng):
+    A = csr.rmat(11, 8, seed=6)
+    d = eng.describe(dev(A))
+    deg = np.diff(A.rowptr)
+    assert d["products_aa"] == csr.products(A, "AA")
+    assert d["products_aat"] == csr.products(A, "AAt")
+    assert d["max_deg"] == deg.max()
+    assert abs(d["deg_cv"] - deg.std() / deg.mean()) < 1e-9
+    rows = np.repeat(np.arange(A.n), deg)
+    assert d["bandwidth"] == np.abs(rows - A.col).max()
+    S = A.to_scipy()
+    P = S.copy()
+    P.data[:] = 1
+    sym = P.multiply(P.T).nnz / A.nnz
+    assert abs(d["pattern_symmetry"] - sym) < 1e-12
+    L = eng.describe(dev(csr.laplace2d(16)))
+    assert L["pattern_symmetry"] == 1.0 and L["bandwidth"] == 16
+
+
+def test_plan_execute_info_and_caller_buffers(eng):
+    A = csr.erdos_renyi(5000, 10.0, seed=12)
+    p = eng.plan(dev(A), "AA")
+    ref = oracle.multiply(A, "AA")
+    assert p.info["nnz_c"] == len(ref[1])
+    assert p.info["products"] == csr.products(A, "AA")
+    out = p.execute()
+    torch.cuda.synchronize()
+    assert_same(out, ref, "plan/execute")
+    out2 = p.execute()  # a plan can execute again
+    torch.cuda.synchronize()
+    assert_same(out2, ref, "plan/execute twice")
+    p.close()
+
+
+def test_deterministic_repeats(eng):
+    A = csr.rmat(12, 16, seed=9)
+    first = None
+    for _ in range(5):
+        C = eng.multiply(dev(A), "AAt")
+        torch.cuda.synchronize()
+        h = C.to_host()
+        if first is None:
+            first = h
+        else:
+            for a, b in zip(first, h):
+                assert np.array_equal(a.view(np.uint8), b.view(np.uint8))
+
+
+def test_run_ours_record(golden, golden_dir):
+    """spg_run_ours reproduces run_ours: nnz(C) and Σv, Σ|v|, Σv² (here bit-equal
+    to the oracle's sequential checksum, since the values are)."""
+    from appt_spgemm_b200.engine import run_ours
+    A = csr.load_bin(os.path.join(golden_dir, "rmat_s9_ef8.csr"))
+    d = dev(A)
+    for task in TASKS:
+        r = run_ours(task, d.rowptr, d.col, d.val, A.n, A.nnz, 3)
+        cp, ci, cx = oracle.multiply(A, task)
+        assert r.nnz == len(ci)
+        assert (r.s, r.as_, r.sq) == oracle.checksum(cx)
+        assert r.ms > 0
+
+
+def test_cli_protocol(golden_dir):
+    """The CLI prints the reference's __chk / RESULT lines (src/spgemm.cu:223-224),
+    parsed here with the reference sweep's patterns (bench/run_compare.py:30-40)."""
+    path = os.path.join(golden_dir, "banded_500_bw8.csr")
+    A = csr.load_bin(path)
+    for task in TASKS:
+        out = subprocess.run([_capi.CLI_PATH, "banded", path, task, "2"], capture_output=True,
+                             text=True, timeout=120, check=True).stdout
+        chk = re.findall(r"__chk s=(\S+) as=(\S+) sq=(\S+)", out)
+        res = [ln.split(",") for ln in out.splitlines() if ln.startswith("RESULT,")]
+        assert len(chk) == 1 and len(res) == 1
+        f = res[0]
+        cp, ci, cx = oracle.multiply(A, task)
+        assert f[1] == "banded" and f[2] == task and int(f[3]) == A.n and int(f[4]) == A.nnz
+        assert int(f[5]) == len(ci) and float(f[6]) > 0
+        s, a, q = oracle.checksum(cx)
+        for got, want in zip(chk[0], (s, a, q)):
+            assert abs(float(got) - want) <= 1e-6 * max(1.0, abs(want))
+
+
+def test_stencil27_full_size_properties(eng):
+    """The 27-point stencil on 96³ at full size: A·A bit-exact against the
+    oracle, nnz(C) equal to the 5×5×5-stencil count, and the Gram path
+    bit-identical to the plain A·Aᵀ."""
+    A = csr.stencil27(96, seed=2)
+    d = dev(A)
+    C = eng.multiply(d, "AA")
+    torch.cuda.synchronize()
+    s = np.array([3, 4] + [5] * 92 + [4, 3], dtype=np.int64)  # reachable offsets per axis
+    assert C.nnz == int(s.sum() ** 3) == 106496000 or C.nnz == int((s.sum()) ** 3)
+    assert_same(C, oracle.multiply(A, "AA", nthreads=0), "stencil27_96/AA")
+    del C
+    G = eng.multiply(d, "AAtS")
+    P = eng.multiply(d, "AAt")
+    torch.cuda.synchronize()
+    assert G.nnz == P.nnz
+    assert torch.equal(G.rowptr, P.rowptr) and torch.equal(G.col, P.col)
+    assert torch.equal(G.val.view(torch.int64), P.val.view(torch.int64))
