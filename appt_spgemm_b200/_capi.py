@@ -61,7 +61,7 @@ class SpgPlanInfo(Structure):
                 ("products", c_int64), ("products_computed", c_int64),
                 ("max_row_products", c_int64), ("max_row_nnz", c_int64),
                 ("heavy_rows", c_int64), ("workspace_bytes", c_int64),
-                ("output_bytes", c_int64), ("bins_used", c_int32), ("reserved", c_int32)]
+                ("output_bytes", c_int64), ("bins_used", c_int32), ("symmetric_pattern", c_int32)]
 
 
 class SpgDescriptors(Structure):

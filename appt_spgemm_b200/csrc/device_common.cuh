@@ -177,6 +177,49 @@ __device__ __forceinline__ void bitonic_sort_keys(const Grp& g, int* keys, int P
   }
 }
 
+// ---- bitonic sort in registers -----------------------------------------------
+// Sorts the 32·E values held by a full warp, E per lane in blocked layout
+// (lane l holds elements l·E … l·E+E−1), ascending.  Partners closer than E
+// are in the same lane (register exchange); farther ones are one shuffle away.
+template <int E, typename U>
+__device__ __forceinline__ void warp_bitonic_sort(U (&r)[E]) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 2; k <= 32 * E; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      if (j >= E) {
+        // partner in lane ^ (j/E); k > j >= E, so both direction bits of
+        // element lane·E + i are bits of the lane: one decision per stage
+        const bool asc = ((lane * E) & k) == 0;
+        const bool lower = (lane & (j / E)) == 0;
+        const bool keep_min = asc == lower;
+#pragma unroll
+        for (int i = 0; i < E; ++i) {
+          const U other = __shfl_xor_sync(0xffffffffu, r[i], j / E);
+          const U mn = r[i] < other ? r[i] : other;
+          const U mx = r[i] < other ? other : r[i];
+          r[i] = keep_min ? mn : mx;
+        }
+      } else {
+        // partner in the same lane; element index bits below E come from i
+        const bool lane_asc = ((lane * E) & k) == 0;
+#pragma unroll
+        for (int i = 0; i < E; ++i) {
+          if ((i & j) == 0) {
+            const bool asc = (k < E) ? ((i & k) == 0) : lane_asc;
+            const U x = r[i], y = r[i + j];
+            const U mn = x < y ? x : y;
+            const U mx = x < y ? y : x;
+            r[i] = asc ? mn : mx;
+            r[i + j] = asc ? mx : mn;
+          }
+        }
+      }
+    }
+  }
+}
+
 __host__ __device__ __forceinline__ int next_pow2_int(int x) {
   int p = 1;
   while (p < x) p <<= 1;

@@ -201,16 +201,26 @@ spg_status check_matrix(const spg_csr_dev* A) {
 }
 
 // Validate A on the device and wait for the verdict (host sync #1).
-spg_status validate_device(spg_ctx* ctx, const MatView& A, cudaStream_t st) {
-  TRY_CUDA(cudaMemsetAsync(ctx->d_status, 0, sizeof(uint32_t), st), "status reset");
+// When sym_tval is given, the values of Aᵀ for a structurally symmetric A are
+// gathered in the same round trip and *symmetric tells whether that held.
+spg_status validate_device(spg_ctx* ctx, const MatView& A, cudaStream_t st,
+                           double* sym_tval = nullptr, bool* symmetric = nullptr) {
+  TRY_CUDA(cudaMemsetAsync(ctx->d_status, 0, 2 * sizeof(uint32_t), st), "status reset");
   {
     ProfScope ps(ctx, "plan/validate", st);
     TRY_CUDA(launch_validate(A, ctx->d_status, st), "validate");
   }
-  TRY_CUDA(cudaMemcpyAsync(ctx->h_pin, ctx->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, st),
-           "status readback");
+  if (sym_tval) {
+    ProfScope ps(ctx, "plan/transpose_sym", st);
+    TRY_CUDA(launch_sym_transpose_vals(A, sym_tval, (int*)(ctx->d_status + 1), st),
+             "symmetric transpose");
+  }
+  TRY_CUDA(cudaMemcpyAsync(ctx->h_pin, ctx->d_status, 2 * sizeof(uint32_t),
+                           cudaMemcpyDeviceToHost, st), "status readback");
   TRY_CUDA(cudaStreamSynchronize(st), "validate sync");
-  return status_from_bits(*(uint32_t*)ctx->h_pin);
+  const uint32_t* h = (const uint32_t*)ctx->h_pin;
+  if (symmetric) *symmetric = h[1] == 0;
+  return status_from_bits(h[0]);
 }
 
 void plan_free(spg_plan* p) {
@@ -233,17 +243,21 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
   p->info.n = n;
   p->info.task = p->task;
   p->info.nnz_a = Ad->nnz;
-  TRY(validate_device(ctx, p->A, st));
-
-  // B = A, or Aᵀ by the counting-sort transpose
+  // B = A; or Aᵀ: for a structurally symmetric A only its values move (gathered
+  // during validation), otherwise the counting-sort transpose builds it
+  double* bx = nullptr;
+  bool symmetric = false;
+  if (p->task != SPG_TASK_AA) TRY(palloc(p, &bx, Ad->nnz));
+  TRY(validate_device(ctx, p->A, st, bx, bx ? &symmetric : nullptr));
+  p->info.symmetric_pattern = symmetric ? 1 : 0;
   if (p->task == SPG_TASK_AA) {
     p->B = p->A;
+  } else if (symmetric) {
+    p->B = MatView{n, Ad->nnz, Ad->rowptr, Ad->col, bx};
   } else {
     int32_t *bp, *bi;
-    double* bx;
     TRY(palloc(p, &bp, (int64_t)n + 1));
     TRY(palloc(p, &bi, Ad->nnz));
-    TRY(palloc(p, &bx, Ad->nnz));
     TransposeWork w{};
     void* scan_tmp;
     TRY(palloc(p, &w.cnt, n));
@@ -315,6 +329,8 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
   ra.rownnz = p->rownnz;
   ra.rowlow = p->rowlow;
   ra.status = ctx->d_status;
+  ra.lo = p->lo;
+  ra.hi = p->hi;
   int bins_used = 0;
   for (int b = 1; b <= kNumTableBins; ++b) {
     if (sym_count[b] == 0) continue;
@@ -431,6 +447,8 @@ spg_status execute_impl(spg_plan* p, spg_csr_out* C, cudaStream_t st) {
     ra.ccol = C->col;
     ra.cval = C->val;
     ra.status = ctx->d_status;
+    ra.lo = p->lo;
+    ra.hi = p->hi;
     if (gram) {
       void *cur, *lc, *lv;
       if ((result = talloc(&cur, sizeof(int32_t) * (size_t)n)) != SPG_OK) break;

@@ -284,6 +284,8 @@ static cudaError_t launch_mode(int bin, const RowArgs& a, int num_sms, cudaStrea
 cudaError_t launch_hash_bin(int bin, bool numeric, bool gram, const RowArgs& a, int num_sms,
                             cudaStream_t s) {
   if (a.nrows <= 0) return cudaSuccess;
+  const int lg = bin + kMinTableLog2 - 1;
+  if (a.G == 32 && lg >= 6 && lg <= 10) return launch_hash_w32(lg, numeric, gram, a, num_sms, s);
   if (numeric) return gram ? launch_mode<true, true>(bin, a, num_sms, s)
                            : launch_mode<true, false>(bin, a, num_sms, s);
   return gram ? launch_mode<false, true>(bin, a, num_sms, s)

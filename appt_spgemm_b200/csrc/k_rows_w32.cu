@@ -1,0 +1,365 @@
+// Warp-per-row shared-memory hash kernels (32 lanes per row, tables of 64 to
+// 1024 slots): the path almost every row of banded / FEM-like matrices takes.
+//
+// Per row the warp
+//  - holds up to 32 entries of A's row in registers (k, a_ik, B-row bounds)
+//    and walks them in order as 32-wide segments of B rows, loading segment
+//    s+1 before hashing segment s, so the gather latency overlaps the probes;
+//  - inserts keys with a read-first, CAS-on-empty linear probe; in the numeric
+//    phase the lane that claims a slot stores 0.0 + a·b there and later
+//    segments add to it, one __syncwarp per segment keeping the k order of
+//    every sum (so no value array is cleared per row);
+//  - packs each occupied slot as ((col − lo) << log2T) | slot, sorts the
+//    packed words with a register bitonic network (E words per lane), and
+//    writes columns and the gathered values to the row's CSR slots.
+// Rows whose column span does not fit the packing take the shared-memory pair
+// sort instead.
+#include <climits>
+
+#include "kernels.h"
+
+namespace spg {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+// CAS-first linear probe: one shared atomic per probe, the loop exits on an
+// empty slot (claimed) or on the key itself.  In the numeric phase the value
+// is then 0.0 + v for a freshly claimed slot and slot + v otherwise — a
+// select, not a branch — so no value array is cleared between rows.
+template <int LOG2T, bool NUMERIC>
+__device__ __forceinline__ void insert_acc(int* keys, double* vals, int j, double v,
+                                           uint32_t* status) {
+  constexpr unsigned T = 1u << LOG2T;
+  unsigned h = hash_slot<LOG2T>(j);
+  int old = atomicCAS(keys + h, kEmptyKey, j);
+  unsigned probe = 1;
+  while (old != kEmptyKey && old != j) {
+    if (probe++ == T) {
+      report(status, DEV_ERR_HASH_FULL);
+      return;
+    }
+    h = (h + 1) & (T - 1);
+    old = atomicCAS(keys + h, kEmptyKey, j);
+  }
+  if (NUMERIC) {
+    const double cur = vals[h];
+    vals[h] = __dadd_rn(old == kEmptyKey ? 0.0 : cur, v);
+  }
+}
+
+// Sorted write-out through packed keys; returns false when P needs more
+// registers than supported (caller falls back to the shared pair sort).
+template <int E, int LOG2T, bool GRAM>
+__device__ __forceinline__ void sort_write(const RowArgs& a, int row, int lo, int m, int* keys,
+                                          const double* vals, int64_t base) {
+  const int lane = threadIdx.x & 31;
+  uint32_t r[E];
+  // blocked layout, loaded and stored with vector accesses (conflict-free)
+  uint32_t* kw = (uint32_t*)keys + lane * E;
+  if (E >= 4) {
+#pragma unroll
+    for (int c = 0; c < E / 4; ++c) {
+      const uint4 v = ((const uint4*)kw)[c];
+      r[4 * c] = v.x;
+      r[4 * c + 1] = v.y;
+      r[4 * c + 2] = v.z;
+      r[4 * c + 3] = v.w;
+    }
+  } else if (E == 2) {
+    const uint2 v = *(const uint2*)kw;
+    r[0] = v.x;
+    r[E - 1] = v.y;
+  } else {
+    r[0] = kw[0];
+  }
+#pragma unroll
+  for (int i = 0; i < E; ++i)
+    if (lane * E + i >= m) r[i] = 0xffffffffu;
+  warp_bitonic_sort<E>(r);
+  __syncwarp();
+  if (E >= 4) {
+#pragma unroll
+    for (int c = 0; c < E / 4; ++c)
+      ((uint4*)kw)[c] = make_uint4(r[4 * c], r[4 * c + 1], r[4 * c + 2], r[4 * c + 3]);
+  } else if (E == 2) {
+    *(uint2*)kw = make_uint2(r[0], r[E - 1]);
+  } else {
+    kw[0] = r[0];
+  }
+  __syncwarp();
+  for (int e = lane; e < m; e += 32) {
+    const uint32_t pk = (uint32_t)keys[e];
+    const int j = lo + (int)(pk >> LOG2T);
+    const double v = vals[pk & ((1u << LOG2T) - 1u)];
+    a.ccol[base + e] = j;
+    a.cval[base + e] = v;
+    if (GRAM && j > row) {
+      const int pos = atomicAdd(&a.cursor[j], 1);
+      if (pos < a.low_in[j]) {
+        const int64_t d = a.lowptr[j] + pos;
+        a.lcol[d] = row;
+        a.lval[d] = v;
+      } else {
+        report(a.status, DEV_ERR_OVERFLOW);
+      }
+    }
+  }
+}
+
+// Fallback: compact (key, value) pairs in slot order and bitonic-sort them in
+// shared memory (for rows whose column span exceeds the 32-bit packing).
+template <int LOG2T, bool GRAM>
+__device__ __noinline__ void pair_sort_write(const RowArgs& a, int row, int* keys, double* vals,
+                                             int64_t base, int expect) {
+  constexpr int T = 1 << LOG2T;
+  const int lane = threadIdx.x & 31;
+  int m = 0;
+  for (int c = 0; c < T; c += 32) {
+    const int s = c + lane;
+    const int key = keys[s];
+    const double v = vals[s];
+    const bool occ = key != kEmptyKey;
+    const unsigned bal = __ballot_sync(kFull, occ);
+    const int pos = m + __popc(bal & lanemask_lt());
+    __syncwarp();
+    if (occ) {
+      keys[pos] = key;
+      vals[pos] = v;
+    }
+    m += __popc(bal);
+    __syncwarp();
+  }
+  const int P = next_pow2_int(m);
+  for (int s = m + lane; s < P; s += 32) keys[s] = INT_MAX;
+  __syncwarp();
+  bitonic_sort_pairs(WarpGroup(32), keys, vals, P);
+  if (m > expect) m = expect;
+  for (int t = lane; t < m; t += 32) {
+    const int j = keys[t];
+    const double v = vals[t];
+    a.ccol[base + t] = j;
+    a.cval[base + t] = v;
+    if (GRAM && j > row) {
+      const int pos = atomicAdd(&a.cursor[j], 1);
+      if (pos < a.low_in[j]) {
+        const int64_t d = a.lowptr[j] + pos;
+        a.lcol[d] = row;
+        a.lval[d] = v;
+      } else {
+        report(a.status, DEV_ERR_OVERFLOW);
+      }
+    }
+  }
+}
+
+}  // namespace
+
+template <int LOG2T, bool NUMERIC, bool GRAM>
+__global__ void __launch_bounds__(256, 5) k_hash_w32(RowArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  constexpr int T = 1 << LOG2T;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  unsigned char* base_p = smem + (size_t)w * (NUMERIC ? (size_t)T * 12 : (size_t)T * 4);
+  double* vals = (double*)base_p;
+  int* keys = (int*)(base_p + (NUMERIC ? (size_t)T * 8 : 0));
+
+  for (int r = blockIdx.x * nw + w; r < a.nrows; r += gridDim.x * nw) {
+    const int row = a.rows[r];
+    for (int s = lane * 4; s < T; s += 128) *(int4*)(keys + s) = make_int4(-1, -1, -1, -1);
+    __syncwarp();
+    const int32_t ps = a.A.rowptr[row], pe = a.A.rowptr[row + 1];
+    for (int32_t pb = ps; pb < pe; pb += 32) {
+      const int cnt = min(32, pe - pb);
+      int bs = 0, len = 0;
+      double av = 0.0;
+      if (lane < cnt) {
+        const int32_t k = a.A.col[pb + lane];
+        bs = a.B.rowptr[k];
+        len = a.B.rowptr[k + 1] - bs;
+        if (NUMERIC) av = a.A.val[pb + lane];
+      }
+      constexpr int D = NUMERIC ? 4 : 8;
+      if (__all_sync(kFull, len <= 32)) {
+        // Fast path: every B row of the chunk is one 32-wide segment.  Rows
+        // t0..t0+D−1 are loaded together, then hashed in order.
+        for (int t0 = 0; t0 < cnt; t0 += D) {
+          int jr[D];
+          double br[D], ar[D];
+#pragma unroll
+          for (int d = 0; d < D; ++d) {
+            const int t = t0 + d;
+            const int tb = __shfl_sync(kFull, bs, t & 31);
+            const int tl = __shfl_sync(kFull, len, t & 31);
+            ar[d] = NUMERIC ? __shfl_sync(kFull, av, t & 31) : 0.0;
+            const bool on = t < cnt && lane < tl;
+            jr[d] = on ? a.B.col[tb + lane] : -1;
+            br[d] = (NUMERIC && on) ? a.B.val[tb + lane] : 0.0;
+          }
+#pragma unroll
+          for (int d = 0; d < D; ++d) {
+            const int j = jr[d];
+            if (j >= 0 && !(NUMERIC && GRAM && j < row))
+              insert_acc<LOG2T, NUMERIC>(keys, vals, j, NUMERIC ? __dmul_rn(ar[d], br[d]) : 0.0,
+                                         a.status);
+            if (NUMERIC) __syncwarp();  // k-order of the accumulation
+          }
+        }
+        continue;
+      }
+      // General path: walk 32-wide segments (t, q0) of B row t in order, D at
+      // a time; the loads of a group are issued before any of it is hashed.
+      int t = 0, q0 = 0;
+      int sbs = __shfl_sync(kFull, bs, 0), slen = __shfl_sync(kFull, len, 0);
+      double sa = NUMERIC ? __shfl_sync(kFull, av, 0) : 0.0;
+      while (t < cnt && q0 >= slen) {
+        ++t;
+        if (t < cnt) {
+          sbs = __shfl_sync(kFull, bs, t);
+          slen = __shfl_sync(kFull, len, t);
+          if (NUMERIC) sa = __shfl_sync(kFull, av, t);
+        }
+      }
+      while (t < cnt) {
+        int jr[D];
+        double br[D], ar[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+          jr[d] = -1;
+          br[d] = 0.0;
+          ar[d] = sa;
+          if (t < cnt) {
+            if (q0 + lane < slen) {
+              jr[d] = a.B.col[sbs + q0 + lane];
+              if (NUMERIC) br[d] = a.B.val[sbs + q0 + lane];
+            }
+            q0 += 32;
+            while (t < cnt && q0 >= slen) {
+              ++t;
+              q0 = 0;
+              if (t < cnt) {
+                sbs = __shfl_sync(kFull, bs, t);
+                slen = __shfl_sync(kFull, len, t);
+                if (NUMERIC) sa = __shfl_sync(kFull, av, t);
+              }
+            }
+          }
+        }
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+          const int j = jr[d];
+          if (j >= 0 && !(NUMERIC && GRAM && j < row))
+            insert_acc<LOG2T, NUMERIC>(keys, vals, j, NUMERIC ? __dmul_rn(ar[d], br[d]) : 0.0,
+                                       a.status);
+          if (NUMERIC) __syncwarp();  // k-order of the accumulation
+        }
+      }
+    }
+    __syncwarp();
+
+    if (!NUMERIC) {
+      int c = 0, cl = 0;
+      for (int s = lane * 4; s < T; s += 128) {
+        const int4 k4 = *(const int4*)(keys + s);
+        c += (k4.x != kEmptyKey) + (k4.y != kEmptyKey) + (k4.z != kEmptyKey) + (k4.w != kEmptyKey);
+        if (GRAM)
+          cl += (k4.x != kEmptyKey && k4.x < row) + (k4.y != kEmptyKey && k4.y < row) +
+                (k4.z != kEmptyKey && k4.z < row) + (k4.w != kEmptyKey && k4.w < row);
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        c += __shfl_xor_sync(kFull, c, o);
+        if (GRAM) cl += __shfl_xor_sync(kFull, cl, o);
+      }
+      if (lane == 0) {
+        a.rownnz[row] = c;
+        if (GRAM) a.rowlow[row] = cl;
+      }
+      __syncwarp();
+      continue;
+    }
+
+    const int32_t low = GRAM ? a.low_in[row] : 0;
+    const int expect = a.cnt_in[row] - low;
+    const int64_t base = a.rowptr[row] + low;
+    const int lo = a.lo[row];
+    const bool packs = (int64_t)a.hi[row] - lo < ((int64_t)1 << (32 - LOG2T));
+    if (!packs || expect > 256) {
+      pair_sort_write<LOG2T, GRAM>(a, row, keys, vals, base, expect);
+      __syncwarp();
+      continue;
+    }
+    // compact occupied slots as packed words, in place
+    int m = 0;
+    for (int c = 0; c < T; c += 32) {
+      const int s = c + lane;
+      const int key = keys[s];
+      const bool occ = key != kEmptyKey;
+      const unsigned bal = __ballot_sync(kFull, occ);
+      const int pos = m + __popc(bal & lanemask_lt());
+      __syncwarp();
+      if (occ) keys[pos] = (int)(((uint32_t)(key - lo) << LOG2T) | (uint32_t)s);
+      m += __popc(bal);
+      __syncwarp();
+    }
+    if (m != expect && lane == 0) report(a.status, DEV_ERR_OVERFLOW);
+    if (m > expect) m = expect;
+    const int P = next_pow2_int(m);
+    if (P <= 32) sort_write<1, LOG2T, GRAM>(a, row, lo, m, keys, vals, base);
+    else if (P <= 64) sort_write<2, LOG2T, GRAM>(a, row, lo, m, keys, vals, base);
+    else if (P <= 128) sort_write<4, LOG2T, GRAM>(a, row, lo, m, keys, vals, base);
+    else sort_write<8, LOG2T, GRAM>(a, row, lo, m, keys, vals, base);
+    __syncwarp();
+  }
+}
+
+template <int LOG2T, bool NUMERIC, bool GRAM>
+static cudaError_t launch_w32(const RowArgs& a, int num_sms, cudaStream_t s) {
+  constexpr int T = 1 << LOG2T;
+  auto kernel = k_hash_w32<LOG2T, NUMERIC, GRAM>;
+  const size_t per = NUMERIC ? (size_t)T * 12 : (size_t)T * 4;
+  int rows = 8;  // warps (rows) per CTA
+  while (rows > 1 && per * rows > 64 * 1024) rows >>= 1;
+  const size_t smem = per * rows;
+  cudaError_t e;
+  if (smem > 48 * 1024) {
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           cudaSharedmemCarveoutMaxShared);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, rows * 32, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) per_sm = 1;
+  int64_t grid = (int64_t)per_sm * num_sms;
+  const int64_t need = (a.nrows + rows - 1) / rows;
+  if (grid > need) grid = need;
+  kernel<<<(unsigned)grid, rows * 32, smem, s>>>(a);
+  SPG_COUNT_LAUNCH();
+  return cudaGetLastError();
+}
+
+template <bool NUMERIC, bool GRAM>
+static cudaError_t w32_mode(int log2t, const RowArgs& a, int num_sms, cudaStream_t s) {
+  switch (log2t) {
+    case 6: return launch_w32<6, NUMERIC, GRAM>(a, num_sms, s);
+    case 7: return launch_w32<7, NUMERIC, GRAM>(a, num_sms, s);
+    case 8: return launch_w32<8, NUMERIC, GRAM>(a, num_sms, s);
+    case 9: return launch_w32<9, NUMERIC, GRAM>(a, num_sms, s);
+    case 10: return launch_w32<10, NUMERIC, GRAM>(a, num_sms, s);
+  }
+  return cudaErrorNotSupported;
+}
+
+cudaError_t launch_hash_w32(int log2t, bool numeric, bool gram, const RowArgs& a, int num_sms,
+                            cudaStream_t s) {
+  if (a.nrows <= 0) return cudaSuccess;
+  if (numeric) return gram ? w32_mode<true, true>(log2t, a, num_sms, s)
+                           : w32_mode<true, false>(log2t, a, num_sms, s);
+  return gram ? w32_mode<false, true>(log2t, a, num_sms, s)
+              : w32_mode<false, false>(log2t, a, num_sms, s);
+}
+
+}  // namespace spg

@@ -31,6 +31,55 @@ __global__ void k_transpose_scatter(MatView A, const int32_t* __restrict__ t_row
   }
 }
 
+// Transpose values of a structurally symmetric A: row k of Aᵀ has A's row-k
+// pattern, and Aᵀ[k,i] = A[i,k] is found by binary search for k in row i.
+// Any entry without its mirror sets *asym; the caller then falls back to the
+// counting sort.  Bounds are checked here because the kernel runs before the
+// host has seen the validation verdict.
+__global__ void k_sym_transpose_vals(MatView A, double* __restrict__ t_val, int* asym) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  bool miss = false;
+  for (int64_t k = warp; k < A.n; k += nwarps) {
+    const int32_t s = A.rowptr[k], e = A.rowptr[k + 1];
+    if (s < 0 || e < s || (int64_t)e > A.nnz) {
+      miss = true;
+      continue;
+    }
+    for (int32_t p = s + lane; p < e; p += 32) {
+      const int32_t i = A.col[p];
+      if (i < 0 || i >= A.n) {
+        miss = true;
+        continue;
+      }
+      int32_t lo = A.rowptr[i], hi = A.rowptr[i + 1];
+      if (lo < 0 || hi < lo || (int64_t)hi > A.nnz) {
+        miss = true;
+        continue;
+      }
+      const int32_t end = hi;
+      while (lo < hi) {
+        const int32_t mid = (lo + hi) >> 1;
+        if (A.col[mid] < k) lo = mid + 1; else hi = mid;
+      }
+      if (lo < end && A.col[lo] == k) t_val[p] = A.val[lo];
+      else miss = true;
+    }
+  }
+  if (__any_sync(0xffffffffu, miss) && lane == 0) atomicOr(asym, 1);
+}
+
+cudaError_t launch_sym_transpose_vals(const MatView& A, double* t_val, int* asym,
+                                      cudaStream_t s) {
+  if (A.n == 0 || A.nnz == 0) return cudaSuccess;
+  int64_t blocks = ((int64_t)A.n * 32 + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  k_sym_transpose_vals<<<(unsigned)blocks, 256, 0, s>>>(A, t_val, asym);
+  SPG_COUNT_LAUNCH();
+  return cudaGetLastError();
+}
+
 // ---- segment sort --------------------------------------------------------------
 constexpr int kShortSeg = 256;      // warp + shared bitonic
 constexpr int kMidSeg = 8192;       // CTA + shared bitonic
@@ -47,7 +96,30 @@ __device__ __forceinline__ int64_t seg_len(const SegSortArgs& a, int64_t s) {
   return a.lens ? (int64_t)a.lens[s] : seg_src(a, s + 1) - seg_src(a, s);
 }
 
-__global__ void __launch_bounds__(256) k_segsort_short(SegSortArgs a) {
+// One segment of at most 32·E entries by one warp: (key << 8 | index) words
+// sorted in registers, then keys written and payloads gathered by index.
+template <int E>
+__device__ __forceinline__ void seg_reg_sort(const SegSortArgs& a, int64_t so, int64_t dof,
+                                             int len) {
+  const int lane = threadIdx.x & 31;
+  uint32_t r[E];
+#pragma unroll
+  for (int i = 0; i < E; ++i) {
+    const int e = lane * E + i;
+    r[i] = e < len ? (((uint32_t)a.src_key[so + e] << 8) | (uint32_t)e) : 0xffffffffu;
+  }
+  warp_bitonic_sort<E>(r);
+#pragma unroll
+  for (int i = 0; i < E; ++i) {
+    const int e = lane * E + i;
+    if (e < len) {
+      a.dst_key[dof + e] = (int32_t)(r[i] >> 8);
+      a.dst_val[dof + e] = a.src_val[so + (r[i] & 255u)];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256, 4) k_segsort_short(SegSortArgs a) {
   __shared__ int skeys[8][kShortSeg];
   __shared__ double svals[8][kShortSeg];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -62,6 +134,13 @@ __global__ void __launch_bounds__(256) k_segsort_short(SegSortArgs a) {
     const int64_t so = seg_src(a, s), dof = seg_dst(a, s);
     if (len > kShortSeg) {
       if (lane == 0) a.long_list[atomicAdd(a.long_count, 1)] = (int32_t)s;
+      continue;
+    }
+    if (a.key_bound <= (1 << 24)) {  // keys fit the (key << 8 | index) packing
+      if (len <= 32) seg_reg_sort<1>(a, so, dof, (int)len);
+      else if (len <= 64) seg_reg_sort<2>(a, so, dof, (int)len);
+      else if (len <= 128) seg_reg_sort<4>(a, so, dof, (int)len);
+      else seg_reg_sort<8>(a, so, dof, (int)len);
       continue;
     }
     const int P = next_pow2_int((int)len);

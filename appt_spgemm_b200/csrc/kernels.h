@@ -110,7 +110,15 @@ struct RowArgs {
   int32_t* lcol;
   double* lval;
   uint32_t* status;
+  // output column span per row (pre-pass): keys of row i lie in [lo[i], hi[i]]
+  const int32_t* lo;
+  const int32_t* hi;
 };
+
+// Warp-per-row kernels (k_rows_w32.cu) for table bins of up to 1024 slots
+// with 32 lanes per row; returns cudaErrorNotSupported for other bins.
+cudaError_t launch_hash_w32(int log2t, bool numeric, bool gram, const RowArgs& a, int num_sms,
+                            cudaStream_t s);
 
 // Launch the kernel of one table bin (1..kNumTableBins).  `gram` selects the
 // A·Aᵀ upper-triangle variant (symbolic: split lower/upper counts; numeric:
@@ -148,6 +156,9 @@ struct TransposeWork {
 };
 cudaError_t launch_transpose(const MatView& A, int32_t* t_rowptr, int32_t* t_col, double* t_val,
                              const TransposeWork& w, int num_sms, cudaStream_t s);
+// Values of Aᵀ for a structurally symmetric A (Aᵀ keeps A's rowptr and col);
+// sets *asym (device int, pre-zeroed) when some entry has no mirror.
+cudaError_t launch_sym_transpose_vals(const MatView& A, double* t_val, int* asym, cudaStream_t s);
 
 // Sort segments of unique int keys (with double payloads) from a source store
 // into a destination store.  Segment s: source [src_off[s], +len), destination

@@ -122,7 +122,7 @@ typedef struct spg_plan_info {
   int64_t workspace_bytes;    /* device workspace held by the plan              */
   int64_t output_bytes;       /* 8(n+1) + 12·nnz_c                              */
   int32_t bins_used;
-  int32_t reserved;
+  int32_t symmetric_pattern;  /* A·Aᵀ tasks: 1 when Aᵀ reused A's pattern      */
 } spg_plan_info;
 
 /* Structural descriptors of A (the reference's dispatcher features,

@@ -170,6 +170,34 @@ def test_transpose_matches_oracle(eng):
         assert np.array_equal(T.val.cpu().numpy(), O.val)
 
 
+def test_transpose_path_selection(eng):
+    """A·Aᵀ reuses A's pattern when it is structurally symmetric (values gathered)
+    and runs the counting-sort transpose otherwise; both give the oracle's C."""
+    for A, sym in ((csr.laplace2d(20), 1), (csr.stencil27(7, seed=3), 1),
+                   (csr.rmat(10, 8, seed=4), 0), (csr.uniform(500, 6, seed=5), 0)):
+        for task in ("AAt", "AAtS"):
+            p = eng.plan(dev(A), task)
+            assert p.info["symmetric_pattern"] == sym
+            out = p.execute()
+            torch.cuda.synchronize()
+            assert_same(out, oracle.multiply(A, task), f"path{sym}/{task}")
+            p.close()
+    # one missing mirror entry forces the general path
+    A = csr.laplace2d(12)
+    keep = np.ones(A.nnz, bool)
+    keep[7] = False
+    rows = np.repeat(np.arange(A.n), np.diff(A.rowptr))[keep]
+    rp = np.zeros(A.n + 1, np.int32)
+    np.cumsum(np.bincount(rows, minlength=A.n), out=rp[1:])
+    B = csr.CsrHost(A.n, rp, A.col[keep].copy(), A.val[keep].copy())
+    p = eng.plan(dev(B), "AAt")
+    assert p.info["symmetric_pattern"] == 0
+    out = p.execute()
+    torch.cuda.synchronize()
+    assert_same(out, oracle.multiply(B, "AAt"), "asymmetric-by-one")
+    p.close()
+
+
 def test_descriptors(eng):
     A = csr.rmat(11, 8, seed=6)
     d = eng.describe(dev(A))
