@@ -100,6 +100,8 @@ SIGNATURES = {
     "spg_profile_read": (c_int32, [_ctx_p, c_char_p, c_uint64]),
     "spg_transpose": (c_int32, [_ctx_p, POINTER(SpgCsrDev), c_void_p, c_void_p, c_void_p,
                                 c_void_p]),
+    "spg_transpose_noalloc": (c_int32, [POINTER(SpgCsrDev), c_void_p, c_void_p, c_void_p,
+                                        c_void_p]),
     "spg_describe": (c_int32, [_ctx_p, POINTER(SpgCsrDev), POINTER(SpgDescriptors), c_void_p]),
     "spg_run_ours": (c_int32, [c_char_p, c_void_p, c_void_p, c_void_p, c_int32, c_int64,
                                c_int32, POINTER(SpgEngResult)]),

@@ -191,6 +191,21 @@ spg_status spg_profile_read(spg_ctx* ctx, char* json, size_t capacity);
 spg_status spg_transpose(spg_ctx* ctx, const spg_csr_dev* A, int32_t* t_rowptr,
                          int32_t* t_col, double* t_val, void* stream);
 
+/* Transpose that allocates nothing.  No counterpart in the reference.
+ * For callers that may not allocate device memory — applications that carve
+ * all GPU memory up front and forbid libraries from calling cudaMalloc /
+ * cudaFree, or latency-critical paths where an allocation may synchronise the
+ * device.  Same result as spg_transpose; the caller passes A and the outputs
+ * (rowptr n+1, col/val nnz), no context.  Its scratch is a static device array
+ * of about 6.8 MB that every GPU loading the library holds until exit, which
+ * limits A to n <= 65,536 and nnz <= 524,288 (larger inputs: SPG_ERR_UNSUPPORTED).
+ * The first call on each device resolves that array's address (set-up); make
+ * it before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU (different streams, or threads) race.  Validates A and
+ * waits for the verdict, then runs asynchronously on `stream`. */
+spg_status spg_transpose_noalloc(const spg_csr_dev* A, int32_t* t_rowptr, int32_t* t_col,
+                                 double* t_val, void* stream);
+
 /* ---- descriptors ----------------------------------------------------------- */
 spg_status spg_describe(spg_ctx* ctx, const spg_csr_dev* A, spg_descriptors* d,
                         void* stream);
