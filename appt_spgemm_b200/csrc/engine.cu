@@ -165,8 +165,13 @@ spg_config merged_config(const spg_config* user) {
   }
   c.struct_size = sizeof(spg_config);
   if (c.max_smem_slots <= 0) c.max_smem_slots = 8192;
-  if (c.heavy_threads <= 0) c.heavy_threads = 512;
-  if (c.window_bits <= 0) c.window_bits = 1 << 18;
+  if (c.heavy_threads <= 0) c.heavy_threads = 1024;
+  if (c.heavy_threads > 1024) c.heavy_threads = 1024;
+  c.heavy_threads = (c.heavy_threads + 31) / 32 * 32;
+  // windows are whole 4-word groups and fit the shared bitmap (≤ 2^20 bits)
+  if (c.window_bits <= 0) c.window_bits = 1 << 20;
+  if (c.window_bits > (1 << 20)) c.window_bits = 1 << 20;
+  c.window_bits = (c.window_bits + 1023) / 1024 * 1024;
   return c;
 }
 

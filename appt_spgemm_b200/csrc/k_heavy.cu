@@ -23,7 +23,7 @@ constexpr size_t kHeavyScratch = 256;
 size_t heavy_smem_bytes(bool numeric, int threads, int window_bits) {
   const size_t words = (size_t)window_bits / 32;
   size_t b = words * 4 + (size_t)threads * 8 + kHeavyScratch;
-  if (numeric) b += words * 4 + (size_t)threads * 8;
+  if (numeric) b += words + (size_t)threads * 8;  // 4-word group prefixes, staged a_ik
   return b;
 }
 
@@ -99,6 +99,15 @@ __global__ void __launch_bounds__(1024) k_heavy_sym(HeavyArgs h) {
   }
 }
 
+// Rank of bit d inside the window: prefix of its 4-word group plus the bits
+// set below it in that group.
+__device__ __forceinline__ int window_rank(const uint32_t* bm, const int* pre4, long long d) {
+  const int i = (int)(d >> 5), b = (int)(d & 31);
+  int r = pre4[i >> 2];
+  for (int w = i & ~3; w < i; ++w) r += __popc(bm[w]);
+  return r + __popc(bm[i] & ((1u << b) - 1u));
+}
+
 template <bool GRAM>
 __global__ void __launch_bounds__(1024) k_heavy_num(HeavyArgs h) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -106,11 +115,12 @@ __global__ void __launch_bounds__(1024) k_heavy_num(HeavyArgs h) {
   const int nw_max = h.window_bits / 32;
   const int HT = blockDim.x;
   uint32_t* bm = (uint32_t*)smem;
-  int* pre = (int*)(bm + nw_max);
-  double* st_a = (double*)(pre + nw_max);
+  int* pre4 = (int*)(bm + nw_max);
+  double* st_a = (double*)(pre4 + nw_max / 4);
   int* st_bs = (int*)(st_a + HT);
   int* st_ex = st_bs + HT;
   void* scratch = (void*)(st_ex + HT);
+  const int tid = threadIdx.x;
   for (int r = blockIdx.x; r < a.nrows; r += gridDim.x) {
     const int row = a.rows[r];
     const int hi = h.hi[row];
@@ -121,57 +131,81 @@ __global__ void __launch_bounds__(1024) k_heavy_num(HeavyArgs h) {
     long long written = 0;
     for (long long w0 = lo; w0 <= hi; w0 += h.window_bits) {
       const int nwords = (int)min((long long)nw_max, (hi - w0) / 32 + 1);
-      for (int i = threadIdx.x; i < nwords; i += HT) bm[i] = 0u;
+      const int ngroups = (nwords + 3) >> 2;
+      for (int i = tid; i < ngroups * 4; i += HT) bm[i] = 0u;
       __syncthreads();
       mark_window(a, row, w0, nwords, bm, st_bs, st_ex, scratch);
-      // per-word exclusive prefix of the bit counts
-      const int per = (nwords + HT - 1) / HT;
-      const int wb = min(nwords, (int)threadIdx.x * per), we = min(nwords, wb + per);
+      // exclusive prefix of the bit counts per group of 4 words
+      const int per = (ngroups + HT - 1) / HT;
+      const int gb = min(ngroups, tid * per), ge = min(ngroups, gb + per);
       int local = 0;
-      for (int i = wb; i < we; ++i) local += __popc(bm[i]);
+      for (int g = gb; g < ge; ++g)
+        local += __popc(bm[4 * g]) + __popc(bm[4 * g + 1]) + __popc(bm[4 * g + 2]) +
+                 __popc(bm[4 * g + 3]);
       int tot;
       int run = block_exclusive_scan(local, (int*)scratch, &tot);
-      for (int i = wb; i < we; ++i) {
-        pre[i] = run;
-        run += __popc(bm[i]);
-      }
       // sorted column indices and zeroed values into the row's CSR slots
-      for (int i = wb; i < we; ++i) {
-        uint32_t wd = bm[i];
-        int rk = pre[i];
-        while (wd) {
-          const int b = __ffs(wd) - 1;
-          wd &= wd - 1u;
-          const long long pos = written + rk;
-          if (pos < expect) {
-            a.ccol[base + pos] = (int32_t)(w0 + 32LL * i + b);
-            a.cval[base + pos] = 0.0;
+      for (int g = gb; g < ge; ++g) {
+        pre4[g] = run;
+        for (int w = 4 * g; w < 4 * g + 4; ++w) {
+          uint32_t wd = bm[w];
+          while (wd) {
+            const int b = __ffs(wd) - 1;
+            wd &= wd - 1u;
+            const long long pos = written + run;
+            if (pos < expect) {
+              a.ccol[base + pos] = (int32_t)(w0 + 32LL * w + b);
+              a.cval[base + pos] = 0.0;
+            }
+            ++run;
           }
-          ++rk;
         }
       }
       __syncthreads();
-      // k-ordered accumulation in place
+      // k-ordered accumulation in place; the first HT entries of B row t+1 are
+      // loaded while row t is accumulated
       const int32_t ps = a.A.rowptr[row], pe = a.A.rowptr[row + 1];
       const long long wbits = (long long)nwords * 32;
       for (int32_t pb = ps; pb < pe; pb += HT) {
         const int cnt = min(HT, pe - pb);
-        if ((int)threadIdx.x < cnt) {
-          const int32_t k = a.A.col[pb + threadIdx.x];
+        if (tid < cnt) {
+          const int32_t k = a.A.col[pb + tid];
           const int32_t bs = a.B.rowptr[k];
-          st_bs[threadIdx.x] = bs;
-          st_ex[threadIdx.x] = a.B.rowptr[k + 1] - bs;
-          st_a[threadIdx.x] = a.A.val[pb + threadIdx.x];
+          st_bs[tid] = bs;
+          st_ex[tid] = a.B.rowptr[k + 1] - bs;
+          st_a[tid] = a.A.val[pb + tid];
         }
         __syncthreads();
+        int jn = -1;
+        double bn = 0.0;
+        if (tid < st_ex[0]) {
+          jn = a.B.col[st_bs[0] + tid];
+          bn = a.B.val[st_bs[0] + tid];
+        }
         for (int t = 0; t < cnt; ++t) {
+          const int j = jn;
+          const double bv = bn;
           const int32_t bs = st_bs[t], len = st_ex[t];
           const double av = st_a[t];
-          for (int q = threadIdx.x; q < len; q += HT) {
+          if (t + 1 < cnt) {
+            jn = -1;
+            if (tid < st_ex[t + 1]) {
+              jn = a.B.col[st_bs[t + 1] + tid];
+              bn = a.B.val[st_bs[t + 1] + tid];
+            }
+          }
+          if (tid < len) {
+            const long long d = (long long)j - w0;
+            if (d >= 0 && d < wbits) {
+              const long long pos = written + window_rank(bm, pre4, d);
+              if (pos < expect)
+                a.cval[base + pos] = __dadd_rn(a.cval[base + pos], __dmul_rn(av, bv));
+            }
+          }
+          for (int q = tid + HT; q < len; q += HT) {
             const long long d = (long long)a.B.col[bs + q] - w0;
             if (d >= 0 && d < wbits) {
-              const int i = (int)(d >> 5), b = (int)(d & 31);
-              const long long pos = written + pre[i] + __popc(bm[i] & ((1u << b) - 1u));
+              const long long pos = written + window_rank(bm, pre4, d);
               if (pos < expect)
                 a.cval[base + pos] = __dadd_rn(a.cval[base + pos], __dmul_rn(av, a.B.val[bs + q]));
             }
@@ -181,10 +215,10 @@ __global__ void __launch_bounds__(1024) k_heavy_num(HeavyArgs h) {
       }
       written += tot;
     }
-    if (written != expect && threadIdx.x == 0) report(a.status, DEV_ERR_OVERFLOW);
+    if (written != expect && tid == 0) report(a.status, DEV_ERR_OVERFLOW);
     if (GRAM) {
       const long long m = written < expect ? written : expect;
-      for (long long t = threadIdx.x; t < m; t += HT) {
+      for (long long t = tid; t < m; t += HT) {
         const int j = a.ccol[base + t];
         if (j > row) {
           const int pos = atomicAdd(&a.cursor[j], 1);

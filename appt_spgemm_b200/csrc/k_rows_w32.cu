@@ -3,17 +3,18 @@
 //
 // Per row the warp
 //  - holds up to 32 entries of A's row in registers (k, a_ik, B-row bounds)
-//    and walks them in order as 32-wide segments of B rows, loading segment
-//    s+1 before hashing segment s, so the gather latency overlaps the probes;
-//  - inserts keys with a read-first, CAS-on-empty linear probe; in the numeric
-//    phase the lane that claims a slot stores 0.0 + a·b there and later
-//    segments add to it, one __syncwarp per segment keeping the k order of
-//    every sum (so no value array is cleared per row);
+//    and walks them in order as 32-wide segments of B rows, loading a group of
+//    D segments before hashing any of them (a branch-light fast path when
+//    every B row of the chunk fits one segment);
+//  - inserts keys with a CAS-first linear probe; in the numeric phase the
+//    lane that claims a slot stores 0.0 + a·b there and later segments add
+//    to it, one __syncwarp per segment keeping the k order of every sum (so
+//    no value array is cleared per row);
 //  - packs each occupied slot as ((col − lo) << log2T) | slot, sorts the
 //    packed words with a register bitonic network (E words per lane), and
 //    writes columns and the gathered values to the row's CSR slots.
-// Rows whose column span does not fit the packing take the shared-memory pair
-// sort instead.
+// Rows whose column span does not fit the packing, or with more than 256
+// entries, take the shared-memory pair sort instead.
 #include <climits>
 
 #include "kernels.h"

@@ -40,34 +40,43 @@ __global__ void k_sym_transpose_vals(MatView A, double* __restrict__ t_val, int*
   const int lane = threadIdx.x & 31;
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  bool miss = false;
   for (int64_t k = warp; k < A.n; k += nwarps) {
+    // once any warp has found an entry without a mirror the result is discarded
+    if (*(volatile int*)asym) break;
+    bool miss = false;
     const int32_t s = A.rowptr[k], e = A.rowptr[k + 1];
     if (s < 0 || e < s || (int64_t)e > A.nnz) {
       miss = true;
-      continue;
+    } else {
+      for (int32_t p = s + lane; p < e; p += 32) {
+        const int32_t i = A.col[p];
+        if (i < 0 || i >= A.n) {
+          miss = true;
+          break;
+        }
+        int32_t lo = A.rowptr[i], hi = A.rowptr[i + 1];
+        if (lo < 0 || hi < lo || (int64_t)hi > A.nnz) {
+          miss = true;
+          break;
+        }
+        const int32_t end = hi;
+        while (lo < hi) {
+          const int32_t mid = (lo + hi) >> 1;
+          if (A.col[mid] < k) lo = mid + 1; else hi = mid;
+        }
+        if (lo < end && A.col[lo] == k) {
+          t_val[p] = A.val[lo];
+        } else {
+          miss = true;
+          break;
+        }
+      }
     }
-    for (int32_t p = s + lane; p < e; p += 32) {
-      const int32_t i = A.col[p];
-      if (i < 0 || i >= A.n) {
-        miss = true;
-        continue;
-      }
-      int32_t lo = A.rowptr[i], hi = A.rowptr[i + 1];
-      if (lo < 0 || hi < lo || (int64_t)hi > A.nnz) {
-        miss = true;
-        continue;
-      }
-      const int32_t end = hi;
-      while (lo < hi) {
-        const int32_t mid = (lo + hi) >> 1;
-        if (A.col[mid] < k) lo = mid + 1; else hi = mid;
-      }
-      if (lo < end && A.col[lo] == k) t_val[p] = A.val[lo];
-      else miss = true;
+    if (__any_sync(0xffffffffu, miss)) {
+      if (lane == 0) atomicOr(asym, 1);
+      break;
     }
   }
-  if (__any_sync(0xffffffffu, miss) && lane == 0) atomicOr(asym, 1);
 }
 
 cudaError_t launch_sym_transpose_vals(const MatView& A, double* t_val, int* asym,
