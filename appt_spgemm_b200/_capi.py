@@ -47,8 +47,9 @@ class SpgCsrOut(Structure):
 class SpgConfig(Structure):
     _fields_ = [("struct_size", c_int32), ("device", c_int32), ("lanes_per_row", c_int32),
                 ("max_smem_slots", c_int32), ("heavy_threads", c_int32),
-                ("window_bits", c_int32), ("force_heavy", c_int32), ("reserved0", c_int32),
-                ("pool_release_bytes", c_int64), ("reserved", c_int64 * 6)]
+                ("window_bits", c_int32), ("force_heavy", c_int32), ("sym_load_pct", c_int32),
+                ("num_load_pct", c_int32), ("reserved0", c_int32),
+                ("pool_release_bytes", c_int64), ("reserved", c_int64 * 5)]
 
 
 class SpgEngResult(Structure):
@@ -95,6 +96,16 @@ SIGNATURES = {
     "spg_multiply": (c_int32, [_ctx_p, c_int32, POINTER(SpgCsrDev), POINTER(SpgCsrOut),
                                c_void_p]),
     "spg_free": (c_int32, [_ctx_p, c_void_p, c_void_p]),
+    "spg_plan_create_batched": (c_int32, [_ctx_p, c_int32, c_int32, POINTER(SpgCsrDev), c_void_p,
+                                          POINTER(_plan_p)]),
+    "spg_plan_batch_offsets": (c_int32, [_plan_p, POINTER(c_int64), POINTER(c_int64)]),
+    "spg_graph_capture": (c_int32, [_plan_p, POINTER(SpgCsrOut), c_void_p, POINTER(c_void_p)]),
+    "spg_graph_launch": (c_int32, [c_void_p, c_void_p]),
+    "spg_graph_destroy": (c_int32, [c_void_p]),
+    "spg_set_config": (c_int32, [_ctx_p, POINTER(SpgConfig)]),
+    "spg_get_config": (c_int32, [_ctx_p, POINTER(SpgConfig)]),
+    "spg_autotune": (c_int32, [_ctx_p, c_int32, c_int32, POINTER(SpgCsrDev), c_int32,
+                               POINTER(SpgConfig), c_void_p]),
     "spg_profile_enable": (c_int32, [_ctx_p, c_int32]),
     "spg_profile_reset": (c_int32, [_ctx_p]),
     "spg_profile_read": (c_int32, [_ctx_p, c_char_p, c_uint64]),

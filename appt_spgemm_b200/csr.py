@@ -130,6 +130,28 @@ def uniform(n: int, per_row: int, seed: int) -> CsrHost:
     return _take(h)
 
 
+def batch_mix(count: int = 512, seed: int = 4, n_min: int = 1000, n_max: int = 64000):
+    """The batched workload: `count` matrices with n = floor(exp(U(ln n_min,
+    ln n_max))); even indices random banded (half-bandwidth U{3..64}, 30%
+    in-band fill), odd indices Erdős–Rényi (row nnz ~ Poisson(λ), λ ~ U(4, 32));
+    values uniform(−1, 1).  Parameters come from numpy's PCG64(seed); each
+    matrix gets its own generator seed.  Returns (matrices, parameter dicts)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    mats, params = [], []
+    for b in range(count):
+        n = int(np.floor(np.exp(rng.uniform(np.log(n_min), np.log(n_max)))))
+        sub = int(rng.integers(0, 2**63 - 1))
+        if b % 2 == 0:
+            bw = int(rng.integers(3, 65))
+            mats.append(banded(n, bw, 0.3, sub))
+            params.append({"kind": "banded", "n": n, "bw": bw, "seed": sub})
+        else:
+            lam = float(rng.uniform(4.0, 32.0))
+            mats.append(erdos_renyi(n, lam, sub))
+            params.append({"kind": "er", "n": n, "lambda": lam, "seed": sub})
+    return mats, params
+
+
 def products(A: CsrHost, task: str) -> int:
     """Intermediate products: A·A Σ_{(i,k)} nnz(A_k); A·Aᵀ Σ_k colcount(k)²
     (est_outputs, bench/run_baseline.py:38-44)."""

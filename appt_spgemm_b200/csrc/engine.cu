@@ -16,6 +16,7 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <algorithm>
 #include <vector>
 
 #include "kernels.h"
@@ -120,9 +121,37 @@ struct spg_plan {
   std::vector<void*> ptrs;
   int64_t ws_bytes = 0;
   cudaEvent_t exec_done = nullptr;
+  // batched plans: instance offsets in the block-diagonal layout
+  int32_t count = 0;
+  const int32_t* colbase = nullptr;
+  std::vector<int64_t> row_off, nnz_off;
+  const BatchDesc* d_desc = nullptr;       // instance table on the device
+  const int64_t* d_nnz_off = nullptr;
+  double* batch_val = nullptr;             // values of the block-diagonal copy
+  // A·Aᵀ: how B's values were derived, to redo it when A's values change
+  bool symmetric = false;
+  TransposeWork tw{};
+  int32_t *bt_rowptr = nullptr, *bt_col = nullptr;
+  double* bt_val = nullptr;
+  // derived values (block-diagonal copy, Aᵀ) still match A: true right after
+  // planning; every later execute recomputes them from A's current values
+  bool values_fresh = true;
+};
+
+struct spg_graph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
 };
 
 namespace {
+
+// Entry of every device-facing call: clear the thread's last error text and a
+// pending non-sticky CUDA error left by earlier, unrelated runtime calls, so
+// that launch checks below report only this call's failures.
+void begin_call() {
+  clear_error();
+  cudaGetLastError();
+}
 
 spg_status cuda_status(cudaError_t e, const char* what) {
   if (e == cudaSuccess) return SPG_OK;
@@ -172,6 +201,12 @@ spg_config merged_config(const spg_config* user) {
   if (c.window_bits <= 0) c.window_bits = 1 << 20;
   if (c.window_bits > (1 << 20)) c.window_bits = 1 << 20;
   c.window_bits = (c.window_bits + 1023) / 1024 * 1024;
+  auto clamp_pct = [](int32_t v, int32_t dflt) { return v <= 0 ? dflt : (v < 20 ? 20 : (v > 90 ? 90 : v)); };
+  c.sym_load_pct = clamp_pct(c.sym_load_pct, 75);
+  c.num_load_pct = clamp_pct(c.num_load_pct, 66);
+  if (c.lanes_per_row != 0 && c.lanes_per_row != 4 && c.lanes_per_row != 8 &&
+      c.lanes_per_row != 16 && c.lanes_per_row != 32)
+    c.lanes_per_row = 0;
   return c;
 }
 
@@ -255,6 +290,8 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
   if (p->task != SPG_TASK_AA) TRY(palloc(p, &bx, Ad->nnz));
   TRY(validate_device(ctx, p->A, st, bx, bx ? &symmetric : nullptr));
   p->info.symmetric_pattern = symmetric ? 1 : 0;
+  p->symmetric = symmetric;
+  p->bt_val = bx;
   if (p->task == SPG_TASK_AA) {
     p->B = p->A;
   } else if (symmetric) {
@@ -277,6 +314,9 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
     ProfScope ps(ctx, "plan/transpose", st);
     TRY_CUDA(launch_transpose(p->A, bp, bi, bx, w, ctx->num_sms, st), "transpose");
     p->B = MatView{n, Ad->nnz, bp, bi, bx};
+    p->tw = w;
+    p->bt_rowptr = bp;
+    p->bt_col = bi;
   }
 
   // lanes per row in the sub-warp bins: next power of two of B's mean row length
@@ -305,7 +345,8 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
   TRY(palloc(p, &counts, 4 * kNumBins));
   TRY(palloc(p, &rows_sym, n));
   const int force = ctx->cfg.force_heavy ? 1 : 0;
-  BinSource bsym{0, n, p->f, p->lo, p->hi, nullptr, nullptr, kMaxTableLog2, force};
+  BinSource bsym{0, n, p->f, p->lo, p->hi, nullptr, nullptr, kMaxTableLog2, force,
+                 ctx->cfg.sym_load_pct};
   {
     ProfScope ps(ctx, "plan/bin_sym", st);
     TRY_CUDA(launch_bin_rows(bsym, hist, counts, rows_sym, st), "symbolic binning");
@@ -378,7 +419,8 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
   // numeric binning by exact counts, stats; host sync #3 (nnz(C))
   TRY(palloc(p, &p->rows_num, n));
   const int num_lg = table_log2_cap(ctx->cfg.max_smem_slots);
-  BinSource bnum{1, n, p->f, p->lo, p->hi, p->rownnz, gram ? p->rowlow : nullptr, num_lg, force};
+  BinSource bnum{1, n, p->f, p->lo, p->hi, p->rownnz, gram ? p->rowlow : nullptr, num_lg, force,
+                 ctx->cfg.num_load_pct};
   {
     ProfScope ps(ctx, "plan/bin_num", st);
     TRY_CUDA(launch_bin_rows(bnum, hist, counts + 2 * kNumBins, p->rows_num, st),
@@ -433,6 +475,28 @@ spg_status execute_impl(spg_plan* p, spg_csr_out* C, cudaStream_t st) {
   TRY_CUDA(cudaSetDevice(ctx->device), "set device");
   TRY_CUDA(cudaMemcpyAsync(C->rowptr, p->rowptr, sizeof(int64_t) * ((size_t)n + 1),
                            cudaMemcpyDeviceToDevice, st), "rowptr copy");
+  // The plan fixed the structure; A's values may have changed since.  Unless
+  // this is the first execute after planning, recompute the values derived
+  // from A (the block-diagonal copy of a batch, the values of Aᵀ).
+  if (!p->values_fresh) {
+    if (p->count > 0) {
+      ProfScope ps(ctx, "exec/batch_vals", st);
+      TRY_CUDA(launch_batch_vals(p->d_desc, p->d_nnz_off, p->count, p->A.nnz, p->batch_val,
+                                 ctx->num_sms, st), "batch values");
+    }
+    if (p->task != SPG_TASK_AA) {
+      ProfScope ps(ctx, "exec/transpose_vals", st);
+      if (p->symmetric) {
+        TRY_CUDA(cudaMemsetAsync(ctx->d_status + 1, 0, sizeof(uint32_t), st), "memset");
+        TRY_CUDA(launch_sym_transpose_vals(p->A, p->bt_val, (int*)(ctx->d_status + 1), st),
+                 "transpose values");
+      } else {
+        TRY_CUDA(launch_transpose(p->A, p->bt_rowptr, p->bt_col, p->bt_val, p->tw, ctx->num_sms,
+                                  st), "transpose");
+      }
+    }
+  }
+  p->values_fresh = false;
   std::vector<void*> tmp;
   auto talloc = [&](void** ptr, size_t bytes) -> spg_status {
     cudaError_t e = cudaMallocFromPoolAsync(ptr, bytes ? bytes : 1, ctx->pool, st);
@@ -454,6 +518,7 @@ spg_status execute_impl(spg_plan* p, spg_csr_out* C, cudaStream_t st) {
     ra.status = ctx->d_status;
     ra.lo = p->lo;
     ra.hi = p->hi;
+    ra.colbase = p->colbase;
     if (gram) {
       void *cur, *lc, *lv;
       if ((result = talloc(&cur, sizeof(int32_t) * (size_t)n)) != SPG_OK) break;
@@ -513,8 +578,15 @@ spg_status execute_impl(spg_plan* p, spg_csr_out* C, cudaStream_t st) {
   } while (0);
   for (void* ptr : tmp) cudaFreeAsync(ptr, st);
   if (result != SPG_OK) return result;
-  if (!p->exec_done) TRY_CUDA(cudaEventCreateWithFlags(&p->exec_done, cudaEventDisableTiming), "event");
-  TRY_CUDA(cudaEventRecord(p->exec_done, st), "event record");
+  // the plan's workspace must outlive this execution: plan_free waits for this
+  // event (not recorded while capturing a graph, whose launches the caller orders)
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  TRY_CUDA(cudaStreamIsCapturing(st, &cap), "capture status");
+  if (cap == cudaStreamCaptureStatusNone) {
+    if (!p->exec_done)
+      TRY_CUDA(cudaEventCreateWithFlags(&p->exec_done, cudaEventDisableTiming), "event");
+    TRY_CUDA(cudaEventRecord(p->exec_done, st), "event record");
+  }
   return SPG_OK;
 }
 
@@ -532,7 +604,7 @@ spg_task parse_task(const char* t, bool* ok) {
 extern "C" {
 
 spg_status spg_create(spg_ctx** out, const spg_config* cfg) {
-  clear_error();
+  begin_call();
   if (!out) return set_error(SPG_ERR_INVALID_ARG, "null context pointer");
   *out = nullptr;
   spg_ctx* ctx = new spg_ctx();
@@ -574,7 +646,7 @@ spg_status spg_create(spg_ctx** out, const spg_config* cfg) {
 }
 
 spg_status spg_destroy(spg_ctx* ctx) {
-  clear_error();
+  begin_call();
   if (!ctx) return SPG_OK;
   cudaSetDevice(ctx->device);
   cudaDeviceSynchronize();
@@ -588,7 +660,7 @@ spg_status spg_destroy(spg_ctx* ctx) {
 }
 
 spg_status spg_check_device_status(spg_ctx* ctx, void* stream) {
-  clear_error();
+  begin_call();
   if (!ctx) return set_error(SPG_ERR_INVALID_ARG, "null context");
   cudaStream_t st = (cudaStream_t)stream;
   TRY_CUDA(cudaMemcpyAsync(ctx->h_pin, ctx->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, st),
@@ -601,7 +673,7 @@ spg_status spg_check_device_status(spg_ctx* ctx, void* stream) {
 
 spg_status spg_plan_create(spg_ctx* ctx, spg_task task, const spg_csr_dev* A, void* stream,
                            spg_plan** out) {
-  clear_error();
+  begin_call();
   if (!ctx || !out) return set_error(SPG_ERR_INVALID_ARG, "null context or plan pointer");
   *out = nullptr;
   if (task != SPG_TASK_AA && task != SPG_TASK_AAT && task != SPG_TASK_AATS)
@@ -624,29 +696,301 @@ spg_status spg_plan_create(spg_ctx* ctx, spg_task task, const spg_csr_dev* A, vo
 }
 
 spg_status spg_plan_get_info(const spg_plan* plan, spg_plan_info* info) {
-  clear_error();
+  begin_call();
   if (!plan || !info) return set_error(SPG_ERR_INVALID_ARG, "null argument");
   *info = plan->info;
   return SPG_OK;
 }
 
 spg_status spg_execute(spg_plan* plan, spg_csr_out* C, void* stream) {
-  clear_error();
+  begin_call();
   if (!plan) return set_error(SPG_ERR_INVALID_ARG, "null plan");
   return execute_impl(plan, C, (cudaStream_t)stream);
 }
 
 spg_status spg_plan_destroy(spg_plan* plan) {
-  clear_error();
+  begin_call();
   if (!plan) return SPG_OK;
   cudaSetDevice(plan->ctx->device);
   plan_free(plan);
   return SPG_OK;
 }
 
+spg_status spg_plan_create_batched(spg_ctx* ctx, spg_task task, int32_t count,
+                                   const spg_csr_dev* As, void* stream, spg_plan** out) {
+  begin_call();
+  if (!ctx || !out || !As || count < 1)
+    return set_error(SPG_ERR_INVALID_ARG, "null argument or count < 1");
+  *out = nullptr;
+  if (task != SPG_TASK_AA && task != SPG_TASK_AAT && task != SPG_TASK_AATS)
+    return set_error(SPG_ERR_INVALID_ARG, "unknown task %d", (int)task);
+  std::vector<BatchDesc> desc((size_t)count);
+  std::vector<int64_t> row_off((size_t)count + 1, 0), nnz_off((size_t)count + 1, 0);
+  for (int32_t b = 0; b < count; ++b) {
+    spg_status s = check_matrix(&As[b]);
+    if (s != SPG_OK) return set_error(s, "instance %d: %s", b, spg_last_error_string());
+    desc[b] = BatchDesc{As[b].rowptr, As[b].col, As[b].val, As[b].n, 0, As[b].nnz, row_off[b],
+                        nnz_off[b]};
+    row_off[b + 1] = row_off[b] + As[b].n;
+    nnz_off[b + 1] = nnz_off[b] + As[b].nnz;
+  }
+  const int64_t N = row_off[count], NNZ = nnz_off[count];
+  if (N > INT32_MAX || NNZ > INT32_MAX)
+    return set_error(SPG_ERR_UNSUPPORTED,
+                     "batch of %lld rows / %lld entries exceeds the int32 block-diagonal layout",
+                     (long long)N, (long long)NNZ);
+  TRY_CUDA(cudaSetDevice(ctx->device), "set device");
+  spg_plan* p = new spg_plan();
+  p->ctx = ctx;
+  p->task = task;
+  p->stream = (cudaStream_t)stream;
+  p->count = count;
+  p->row_off = row_off;
+  cudaStream_t st = p->stream;
+  spg_status s = SPG_OK;
+  int32_t *rp = nullptr, *col = nullptr, *cb = nullptr;
+  double* val = nullptr;
+  BatchDesc* d_desc = nullptr;
+  int64_t *d_row_off = nullptr, *d_nnz_off = nullptr, *d_cnnz_off = nullptr;
+  do {
+    if ((s = palloc(p, &rp, N + 1)) != SPG_OK) break;
+    if ((s = palloc(p, &col, NNZ)) != SPG_OK) break;
+    if ((s = palloc(p, &val, NNZ)) != SPG_OK) break;
+    if ((s = palloc(p, &cb, N)) != SPG_OK) break;
+    if ((s = palloc(p, &d_desc, count)) != SPG_OK) break;
+    if ((s = palloc(p, &d_row_off, (int64_t)count + 1)) != SPG_OK) break;
+    if ((s = palloc(p, &d_nnz_off, (int64_t)count + 1)) != SPG_OK) break;
+    if ((s = palloc(p, &d_cnnz_off, (int64_t)count + 1)) != SPG_OK) break;
+    cudaError_t e = cudaMemcpyAsync(d_desc, desc.data(), sizeof(BatchDesc) * desc.size(),
+                                    cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(d_row_off, row_off.data(), sizeof(int64_t) * row_off.size(),
+                          cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(d_nnz_off, nnz_off.data(), sizeof(int64_t) * nnz_off.size(),
+                          cudaMemcpyHostToDevice, st);
+    // instance checks report into status word 2 (word 0 is reset by validation)
+    if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_status + 2, 0, sizeof(uint32_t), st);
+    if (e == cudaSuccess) {
+      ProfScope ps(ctx, "plan/batch_concat", st);
+      e = launch_batch_concat(d_desc, d_row_off, d_nnz_off, count, N, NNZ, rp, col, val, cb,
+                              ctx->d_status + 2, ctx->num_sms, st);
+    }
+    if (e != cudaSuccess) { s = cuda_status(e, "batch concatenation"); break; }
+    p->colbase = cb;
+    p->d_desc = d_desc;
+    p->d_nnz_off = d_nnz_off;
+    p->batch_val = val;
+    spg_csr_dev big{(int32_t)N, NNZ, rp, col, val};
+    if ((s = plan_build(p, &big)) != SPG_OK) break;
+    // instance checks and the per-instance C offsets, one more round trip
+    e = launch_gather_offsets(p->rowptr, d_row_off, count, d_cnnz_off, st);
+    std::vector<int64_t> cnnz((size_t)count + 1);
+    uint32_t bad = 0;
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(cnnz.data(), d_cnnz_off, sizeof(int64_t) * cnnz.size(),
+                          cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(&bad, ctx->d_status + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) { s = cuda_status(e, "batch offsets"); break; }
+    if (bad) {
+      s = set_error(SPG_ERR_INVALID_CSR,
+                    "an instance's rowptr does not run from 0 to its nnz, or a column lies "
+                    "outside [0, n) of its instance");
+      break;
+    }
+    p->nnz_off = cnnz;
+  } while (0);
+  if (s != SPG_OK) {
+    cudaStreamSynchronize(st);
+    plan_free(p);
+    return s;
+  }
+  *out = p;
+  return SPG_OK;
+}
+
+spg_status spg_plan_batch_offsets(const spg_plan* plan, int64_t* row_off, int64_t* nnz_off) {
+  begin_call();
+  if (!plan) return set_error(SPG_ERR_INVALID_ARG, "null plan");
+  if (plan->count == 0) return set_error(SPG_ERR_INVALID_ARG, "not a batched plan");
+  if (row_off) std::memcpy(row_off, plan->row_off.data(), sizeof(int64_t) * plan->row_off.size());
+  if (nnz_off) std::memcpy(nnz_off, plan->nnz_off.data(), sizeof(int64_t) * plan->nnz_off.size());
+  return SPG_OK;
+}
+
+spg_status spg_graph_capture(spg_plan* plan, spg_csr_out* C, void* stream, spg_graph** out) {
+  begin_call();
+  if (!plan || !C || !out) return set_error(SPG_ERR_INVALID_ARG, "null argument");
+  *out = nullptr;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (!st || st == cudaStreamLegacy || st == cudaStreamPerThread)
+    return set_error(SPG_ERR_INVALID_ARG, "graph capture needs a created (non-default) stream");
+  TRY_CUDA(cudaSetDevice(plan->ctx->device), "set device");
+  TRY_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+  plan->values_fresh = false;  // every launch recomputes values derived from A
+  spg_status s = execute_impl(plan, C, st);
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(st, &g);
+  if (s != SPG_OK) {
+    if (g) cudaGraphDestroy(g);
+    return s;
+  }
+  if (e != cudaSuccess) return cuda_status(e, "end capture");
+  cudaGraphExec_t ex = nullptr;
+  e = cudaGraphInstantiate(&ex, g, 0);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return cuda_status(e, "graph instantiate");
+  }
+  spg_graph* gr = new spg_graph();
+  gr->graph = g;
+  gr->exec = ex;
+  *out = gr;
+  return SPG_OK;
+}
+
+spg_status spg_graph_launch(spg_graph* graph, void* stream) {
+  begin_call();
+  if (!graph) return set_error(SPG_ERR_INVALID_ARG, "null graph");
+  TRY_CUDA(cudaGraphLaunch(graph->exec, (cudaStream_t)stream), "graph launch");
+  return SPG_OK;
+}
+
+spg_status spg_graph_destroy(spg_graph* graph) {
+  begin_call();
+  if (!graph) return SPG_OK;
+  if (graph->exec) cudaGraphExecDestroy(graph->exec);
+  if (graph->graph) cudaGraphDestroy(graph->graph);
+  delete graph;
+  return SPG_OK;
+}
+
+spg_status spg_set_config(spg_ctx* ctx, const spg_config* cfg) {
+  begin_call();
+  if (!ctx || !cfg) return set_error(SPG_ERR_INVALID_ARG, "null argument");
+  const int dev = ctx->device;
+  ctx->cfg = merged_config(cfg);
+  ctx->cfg.device = dev;
+  return SPG_OK;
+}
+
+spg_status spg_get_config(const spg_ctx* ctx, spg_config* cfg) {
+  begin_call();
+  if (!ctx || !cfg) return set_error(SPG_ERR_INVALID_ARG, "null argument");
+  *cfg = ctx->cfg;
+  return SPG_OK;
+}
+
+namespace {
+
+// One full product (plan, output allocation, execute, release) with the
+// context's current tuning, timed with events on `st`.
+spg_status tune_run(spg_ctx* ctx, spg_task task, int32_t count, const spg_csr_dev* As,
+                    cudaStream_t st, float* ms, int64_t* heavy_rows) {
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  TRY_CUDA(cudaEventCreate(&e0), "event");
+  TRY_CUDA(cudaEventCreate(&e1), "event");
+  cudaEventRecord(e0, st);
+  spg_plan* p = nullptr;
+  spg_status s = count == 1 ? spg_plan_create(ctx, task, As, st, &p)
+                            : spg_plan_create_batched(ctx, task, count, As, st, &p);
+  spg_csr_out C{};
+  if (s == SPG_OK) {
+    if (heavy_rows) *heavy_rows = p->info.heavy_rows;
+    C.n = p->n;
+    const size_t nz = (size_t)(p->nnz_c > 0 ? p->nnz_c : 1);
+    cudaError_t e = cudaMallocFromPoolAsync((void**)&C.rowptr, 8 * ((size_t)p->n + 1), ctx->pool, st);
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync((void**)&C.col, 4 * nz, ctx->pool, st);
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync((void**)&C.val, 8 * nz, ctx->pool, st);
+    s = e == cudaSuccess ? execute_impl(p, &C, st) : cuda_status(e, "autotune output");
+    if (C.rowptr) cudaFreeAsync(C.rowptr, st);
+    if (C.col) cudaFreeAsync(C.col, st);
+    if (C.val) cudaFreeAsync(C.val, st);
+    plan_free(p);
+  }
+  cudaEventRecord(e1, st);
+  cudaEventSynchronize(e1);
+  float t = 0.f;
+  cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms = t;
+  return s;
+}
+
+}  // namespace
+
+spg_status spg_autotune(spg_ctx* ctx, spg_task task, int32_t count, const spg_csr_dev* As,
+                        int32_t reps, spg_config* best, void* stream) {
+  begin_call();
+  if (!ctx || !As || count < 1) return set_error(SPG_ERR_INVALID_ARG, "bad arguments");
+  if (reps < 1) reps = 3;
+  cudaStream_t st = (cudaStream_t)stream;
+  const spg_config start = ctx->cfg;
+  int64_t heavy = 0;
+  auto measure = [&](const spg_config& c, float* out) -> spg_status {
+    ctx->cfg = merged_config(&c);
+    ctx->cfg.device = start.device;
+    float t;
+    spg_status s = tune_run(ctx, task, count, As, st, &t, &heavy);  // warm-up
+    std::vector<float> v;
+    for (int r = 0; r < reps && s == SPG_OK; ++r) {
+      s = tune_run(ctx, task, count, As, st, &t, nullptr);
+      v.push_back(t);
+    }
+    if (s != SPG_OK) return s;
+    std::sort(v.begin(), v.end());
+    *out = v[v.size() / 2];
+    return SPG_OK;
+  };
+  spg_config cur = start;
+  float cur_ms = 0.f;
+  spg_status s = measure(cur, &cur_ms);
+  if (s != SPG_OK) {
+    ctx->cfg = start;
+    return s;
+  }
+  const bool has_heavy = heavy > 0;
+  using Field = int32_t spg_config::*;
+  struct Knob {
+    Field field;
+    std::vector<int32_t> values;
+    bool heavy_only;
+  };
+  const std::vector<Knob> knobs = {
+      {&spg_config::lanes_per_row, {4, 8, 16, 32}, false},
+      {&spg_config::num_load_pct, {40, 50, 66, 80}, false},
+      {&spg_config::sym_load_pct, {50, 75, 90}, false},
+      {&spg_config::max_smem_slots, {2048, 4096, 8192, 16384}, false},
+      {&spg_config::heavy_threads, {256, 512, 1024}, true},
+      {&spg_config::window_bits, {1 << 18, 1 << 19, 1 << 20}, true},
+  };
+  for (const Knob& k : knobs) {
+    if (k.heavy_only && !has_heavy) continue;
+    for (int32_t v : k.values) {
+      if (cur.*(k.field) == v) continue;
+      spg_config c = cur;
+      c.*(k.field) = v;
+      float t = 0.f;
+      if (measure(c, &t) != SPG_OK) continue;  // a candidate that fails is skipped
+      if (t < cur_ms * 0.98f) {
+        cur = merged_config(&c);
+        cur_ms = t;
+      }
+    }
+  }
+  ctx->cfg = merged_config(&cur);
+  ctx->cfg.device = start.device;
+  if (best) *best = ctx->cfg;
+  begin_call();
+  return SPG_OK;
+}
+
 spg_status spg_multiply(spg_ctx* ctx, spg_task task, const spg_csr_dev* A, spg_csr_out* C,
                         void* stream) {
-  clear_error();
+  begin_call();
   if (!C) return set_error(SPG_ERR_INVALID_ARG, "null output");
   spg_plan* p = nullptr;
   TRY(spg_plan_create(ctx, task, A, stream, &p));
@@ -681,7 +1025,7 @@ spg_status spg_multiply(spg_ctx* ctx, spg_task task, const spg_csr_dev* A, spg_c
 }
 
 spg_status spg_free(spg_ctx* ctx, void* dev_ptr, void* stream) {
-  clear_error();
+  begin_call();
   if (!ctx) return set_error(SPG_ERR_INVALID_ARG, "null context");
   if (!dev_ptr) return SPG_OK;
   TRY_CUDA(cudaFreeAsync(dev_ptr, (cudaStream_t)stream), "free");
@@ -690,7 +1034,7 @@ spg_status spg_free(spg_ctx* ctx, void* dev_ptr, void* stream) {
 
 spg_status spg_transpose(spg_ctx* ctx, const spg_csr_dev* A, int32_t* t_rowptr, int32_t* t_col,
                          double* t_val, void* stream) {
-  clear_error();
+  begin_call();
   if (!ctx) return set_error(SPG_ERR_INVALID_ARG, "null context");
   TRY(check_matrix(A));
   if (!t_rowptr || (A->nnz > 0 && (!t_col || !t_val)))
@@ -723,7 +1067,7 @@ spg_status spg_transpose(spg_ctx* ctx, const spg_csr_dev* A, int32_t* t_rowptr, 
 }
 
 spg_status spg_describe(spg_ctx* ctx, const spg_csr_dev* A, spg_descriptors* d, void* stream) {
-  clear_error();
+  begin_call();
   if (!ctx || !d) return set_error(SPG_ERR_INVALID_ARG, "null argument");
   TRY(check_matrix(A));
   TRY_CUDA(cudaSetDevice(ctx->device), "set device");
@@ -773,14 +1117,14 @@ spg_status spg_describe(spg_ctx* ctx, const spg_csr_dev* A, spg_descriptors* d, 
 }
 
 spg_status spg_profile_enable(spg_ctx* ctx, int32_t enable) {
-  clear_error();
+  begin_call();
   if (!ctx) return set_error(SPG_ERR_INVALID_ARG, "null context");
   ctx->prof = enable != 0;
   return SPG_OK;
 }
 
 spg_status spg_profile_reset(spg_ctx* ctx) {
-  clear_error();
+  begin_call();
   if (!ctx) return set_error(SPG_ERR_INVALID_ARG, "null context");
   TRY_CUDA(cudaSetDevice(ctx->device), "set device");
   prof_resolve(ctx);
@@ -790,7 +1134,7 @@ spg_status spg_profile_reset(spg_ctx* ctx) {
 }
 
 spg_status spg_profile_read(spg_ctx* ctx, char* json, size_t capacity) {
-  clear_error();
+  begin_call();
   if (!ctx || !json || capacity == 0) return set_error(SPG_ERR_INVALID_ARG, "bad arguments");
   TRY_CUDA(cudaSetDevice(ctx->device), "set device");
   TRY_CUDA(cudaDeviceSynchronize(), "profile sync");
@@ -813,7 +1157,7 @@ spg_status spg_profile_read(spg_ctx* ctx, char* json, size_t capacity) {
 }
 
 spg_status spg_checksum(const double* dev_val, int64_t count, double* s, double* as, double* sq) {
-  clear_error();
+  begin_call();
   if (!s || !as || !sq || count < 0 || (count > 0 && !dev_val))
     return set_error(SPG_ERR_INVALID_ARG, "bad checksum arguments");
   std::vector<double> h((size_t)count);
@@ -835,7 +1179,7 @@ spg_status spg_checksum(const double* dev_val, int64_t count, double* s, double*
 spg_status spg_run_ours(const char* task, const int32_t* dOff, const int32_t* dCol,
                         const double* dVal, int32_t n, int64_t nnz, int32_t reps,
                         spg_eng_result* out) {
-  clear_error();
+  begin_call();
   bool ok;
   spg_task t = parse_task(task, &ok);
   if (!ok) return set_error(SPG_ERR_INVALID_ARG, "task must be AA, AAt or AAtS");

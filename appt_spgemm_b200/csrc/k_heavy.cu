@@ -128,6 +128,7 @@ __global__ void __launch_bounds__(1024) k_heavy_num(HeavyArgs h) {
     const int32_t low = GRAM ? a.low_in[row] : 0;
     const long long expect = (long long)a.cnt_in[row] - low;
     const int64_t base = a.rowptr[row] + low;
+    const int cb = a.colbase ? a.colbase[row] : 0;
     long long written = 0;
     for (long long w0 = lo; w0 <= hi; w0 += h.window_bits) {
       const int nwords = (int)min((long long)nw_max, (hi - w0) / 32 + 1);
@@ -154,7 +155,7 @@ __global__ void __launch_bounds__(1024) k_heavy_num(HeavyArgs h) {
             wd &= wd - 1u;
             const long long pos = written + run;
             if (pos < expect) {
-              a.ccol[base + pos] = (int32_t)(w0 + 32LL * w + b);
+              a.ccol[base + pos] = (int32_t)(w0 + 32LL * w + b) - cb;
               a.cval[base + pos] = 0.0;
             }
             ++run;
@@ -219,12 +220,12 @@ __global__ void __launch_bounds__(1024) k_heavy_num(HeavyArgs h) {
     if (GRAM) {
       const long long m = written < expect ? written : expect;
       for (long long t = tid; t < m; t += HT) {
-        const int j = a.ccol[base + t];
+        const int j = a.ccol[base + t] + cb;
         if (j > row) {
           const int pos = atomicAdd(&a.cursor[j], 1);
           if (pos < a.low_in[j]) {
             const int64_t d = a.lowptr[j] + pos;
-            a.lcol[d] = row;
+            a.lcol[d] = row - cb;
             a.lval[d] = a.cval[base + t];
           } else {
             report(a.status, DEV_ERR_OVERFLOW);

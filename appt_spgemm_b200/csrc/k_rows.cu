@@ -146,16 +146,17 @@ __device__ __forceinline__ void hash_row(const Grp& g, const RowArgs& a, const i
     if (m > expect) m = expect;
   }
   const int64_t base = a.rowptr[row] + low;
+  const int cb = a.colbase ? a.colbase[row] : 0;
   for (int t = g.lane; t < m; t += g.G) {
     const int j = keys[t];
     const double v = vals[t];
-    a.ccol[base + t] = j;
+    a.ccol[base + t] = j - cb;
     a.cval[base + t] = v;
     if (GRAM && j > row) {
       const int pos = atomicAdd(&a.cursor[j], 1);
       if (pos < a.low_in[j]) {
         const int64_t d = a.lowptr[j] + pos;
-        a.lcol[d] = row;
+        a.lcol[d] = row - cb;
         a.lval[d] = v;
       } else {
         report(a.status, DEV_ERR_OVERFLOW);

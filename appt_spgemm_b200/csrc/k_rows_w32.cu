@@ -90,17 +90,18 @@ __device__ __forceinline__ void sort_write(const RowArgs& a, int row, int lo, in
     kw[0] = r[0];
   }
   __syncwarp();
+  const int cb = a.colbase ? a.colbase[row] : 0;
   for (int e = lane; e < m; e += 32) {
     const uint32_t pk = (uint32_t)keys[e];
     const int j = lo + (int)(pk >> LOG2T);
     const double v = vals[pk & ((1u << LOG2T) - 1u)];
-    a.ccol[base + e] = j;
+    a.ccol[base + e] = j - cb;
     a.cval[base + e] = v;
     if (GRAM && j > row) {
       const int pos = atomicAdd(&a.cursor[j], 1);
       if (pos < a.low_in[j]) {
         const int64_t d = a.lowptr[j] + pos;
-        a.lcol[d] = row;
+        a.lcol[d] = row - cb;
         a.lval[d] = v;
       } else {
         report(a.status, DEV_ERR_OVERFLOW);
@@ -137,16 +138,17 @@ __device__ __noinline__ void pair_sort_write(const RowArgs& a, int row, int* key
   __syncwarp();
   bitonic_sort_pairs(WarpGroup(32), keys, vals, P);
   if (m > expect) m = expect;
+  const int cb = a.colbase ? a.colbase[row] : 0;
   for (int t = lane; t < m; t += 32) {
     const int j = keys[t];
     const double v = vals[t];
-    a.ccol[base + t] = j;
+    a.ccol[base + t] = j - cb;
     a.cval[base + t] = v;
     if (GRAM && j > row) {
       const int pos = atomicAdd(&a.cursor[j], 1);
       if (pos < a.low_in[j]) {
         const int64_t d = a.lowptr[j] + pos;
-        a.lcol[d] = row;
+        a.lcol[d] = row - cb;
         a.lval[d] = v;
       } else {
         report(a.status, DEV_ERR_OVERFLOW);

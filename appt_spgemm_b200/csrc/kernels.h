@@ -38,6 +38,7 @@ struct BinSource {
   const int32_t* rowlow;    // numeric gram: lower-part count (bin uses rownnz − rowlow)
   int max_log2;             // largest shared table (log2 slots) before the heavy path
   int force_heavy;
+  int load_pct;             // table sized for at most this load (percent)
 };
 
 __host__ __device__ __forceinline__ int ceil_log2_64(int64_t x) {
@@ -46,24 +47,23 @@ __host__ __device__ __forceinline__ int ceil_log2_64(int64_t x) {
   return l;
 }
 
-// Table size rule: symbolic tables hold keys only and are sized for load ≤ 3/4
-// of min(products, span); numeric tables hold key+value for load ≤ 2/3 of the
-// exact row count.  Bin b in 1..kNumTableBins means 2^(b+kMinTableLog2−1) slots.
+// Table size rule: symbolic tables hold keys only and are sized for the load
+// limit (default 75%) of min(products, span); numeric tables hold key+value
+// and are sized for the load limit (default 66%) of the exact row count.
+// Bin b in 1..kNumTableBins means 2^(b+kMinTableLog2−1) slots.
 __host__ __device__ __forceinline__ int row_bin(const BinSource& s, int i) {
   int64_t size;
-  int64_t want;
   if (s.mode == 0) {
     int64_t f = s.f[i];
     if (f <= 0) return kEmptyBin;
     int64_t span = (int64_t)s.hi[i] - (int64_t)s.lo[i] + 1;
     size = f < span ? f : span;
-    want = size + size / 3 + 1;
   } else {
     int64_t m = s.rownnz[i] - (s.rowlow ? s.rowlow[i] : 0);
     if (m <= 0) return kEmptyBin;
     size = m;
-    want = m + m / 2 + 1;
   }
+  const int64_t want = size * 100 / s.load_pct + 1;
   if (s.force_heavy) return kHeavyBin;
   int lg = ceil_log2_64(want);
   if (lg < kMinTableLog2) lg = kMinTableLog2;
@@ -113,6 +113,9 @@ struct RowArgs {
   // output column span per row (pre-pass): keys of row i lie in [lo[i], hi[i]]
   const int32_t* lo;
   const int32_t* hi;
+  // batched plans: first column of the row's instance, subtracted from every
+  // column index written (nullptr for a single matrix)
+  const int32_t* colbase;
 };
 
 // Warp-per-row kernels (k_rows_w32.cu) for table bins of up to 1024 slots
@@ -180,6 +183,31 @@ struct SegSortArgs {
   uint32_t* status;
 };
 cudaError_t launch_segsort(const SegSortArgs& a, int num_sms, cudaStream_t s);
+
+// ---- batched plans (k_batch.cu) ---------------------------------------------
+struct BatchDesc {          // one instance, as uploaded to the device
+  const int32_t* rowptr;
+  const int32_t* col;
+  const double* val;
+  int32_t n;
+  int32_t pad;
+  int64_t nnz;
+  int64_t row_off;          // first row (and column) of the instance in the block diagonal
+  int64_t nnz_off;          // first entry of the instance
+};
+// Block-diagonal concatenation: rowptr (N+1), col/val (NNZ) with columns offset
+// by the instance's row_off, colbase[r] = row_off of row r's instance.  Sets
+// *bad when an instance's rowptr does not run 0..nnz or a column leaves its block.
+cudaError_t launch_batch_concat(const BatchDesc* d, const int64_t* row_off, const int64_t* nnz_off,
+                                int count, int64_t N, int64_t NNZ, int32_t* rowptr, int32_t* col,
+                                double* val, int32_t* colbase, uint32_t* bad, int num_sms,
+                                cudaStream_t s);
+// Refresh only the values of the block-diagonal copy from the instances.
+cudaError_t launch_batch_vals(const BatchDesc* d, const int64_t* nnz_off, int count, int64_t NNZ,
+                              double* val, int num_sms, cudaStream_t s);
+// out[b] = rowptr_c[row_off[b]] for b = 0..count.
+cudaError_t launch_gather_offsets(const int64_t* rowptr_c, const int64_t* row_off, int count,
+                                  int64_t* out, cudaStream_t s);
 
 // ---- descriptors ------------------------------------------------------------
 struct DescAccum {        // device accumulators of spg_describe

@@ -106,11 +106,12 @@ def make_config(**kw) -> SpgConfig:
 class Plan:
     """Pre-pass, binning and symbolic phase done; nnz(C) known (``info``)."""
 
-    def __init__(self, engine: "Engine", handle: ctypes.c_void_p, A: CsrDevice, task: str):
+    def __init__(self, engine: "Engine", handle: ctypes.c_void_p, A, task: str, count: int = 0):
         self._engine = engine
         self._h = handle
-        self._A = A  # keep the input alive for execute
+        self._A = A  # keep the input(s) alive for execute
         self.task = task
+        self.count = count
         info = SpgPlanInfo()
         check(lib().spg_plan_get_info(self._h, ctypes.byref(info)), "plan info")
         self.info = {f: getattr(info, f) for f, _ in SpgPlanInfo._fields_ if f != "reserved"}
@@ -121,7 +122,7 @@ class Plan:
 
     def execute(self, out: Optional[CsrResult] = None, stream=None) -> CsrResult:
         n = self.info["n"]
-        dev = self._A.rowptr.device
+        dev = (self._A[0] if isinstance(self._A, (list, tuple)) else self._A).rowptr.device
         if out is None:
             out = CsrResult(
                 n, self.nnz_c,
@@ -138,6 +139,27 @@ class Plan:
         out.nnz = int(c.nnz)
         return out
 
+    def offsets(self):
+        """Batched plans: (row_off, nnz_off) int64 arrays of count+1 entries —
+        instance b owns rows [row_off[b], row_off[b+1]) and entries
+        [nnz_off[b], nnz_off[b+1]) of the concatenated C."""
+        import numpy as np
+        n = self.count + 1
+        ro = np.zeros(n, dtype=np.int64)
+        no = np.zeros(n, dtype=np.int64)
+        check(lib().spg_plan_batch_offsets(self._h, ro.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                           no.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))),
+              "batch offsets")
+        return ro, no
+
+    def capture_graph(self, out: CsrResult, stream: torch.cuda.Stream) -> "Graph":
+        """CUDA graph of execute() into `out` on `stream` (a created stream)."""
+        c = SpgCsrOut(out.n, 0, out.rowptr.data_ptr(), out.col.data_ptr(), out.val.data_ptr())
+        g = ctypes.c_void_p()
+        check(lib().spg_graph_capture(self._h, ctypes.byref(c), int(stream.cuda_stream),
+                                      ctypes.byref(g)), "graph capture")
+        return Graph(g, self, out)
+
     def close(self) -> None:
         if self._h:
             lib().spg_plan_destroy(self._h)
@@ -148,6 +170,45 @@ class Plan:
             self.close()
         except Exception:
             pass
+
+
+class Graph:
+    """An instantiated CUDA graph of one plan's execute phase."""
+
+    def __init__(self, handle, plan: Plan, out: CsrResult):
+        self._h = handle
+        self._plan = plan  # the graph reads the plan's workspace
+        self.out = out
+
+    def launch(self, stream: Optional[torch.cuda.Stream] = None) -> CsrResult:
+        check(lib().spg_graph_launch(self._h, _stream_handle(stream)), "graph launch")
+        return self.out
+
+    def close(self) -> None:
+        if self._h:
+            lib().spg_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class BatchResult:
+    """Concatenated C of a batched product and the instance offsets."""
+
+    C: CsrResult
+    row_off: "object"
+    nnz_off: "object"
+
+    def instance(self, b: int):
+        """(rowptr int64 rebased to 0, col, val) device views of instance b."""
+        r0, r1 = int(self.row_off[b]), int(self.row_off[b + 1])
+        e0, e1 = int(self.nnz_off[b]), int(self.nnz_off[b + 1])
+        return (self.C.rowptr[r0:r1 + 1] - e0, self.C.col[e0:e1], self.C.val[e0:e1])
 
 
 class Engine:
@@ -199,6 +260,48 @@ class Engine:
             return p.execute(stream=stream)
         finally:
             p.close()
+
+    def plan_batched(self, As, task: str = "AA", stream=None) -> Plan:
+        """One plan for many independent products (block-diagonal layout)."""
+        arr = (SpgCsrDev * len(As))(*[A.struct() for A in As])
+        p = ctypes.c_void_p()
+        check(lib().spg_plan_create_batched(self._h, _task_id(task), len(As), arr,
+                                            _stream_handle(stream), ctypes.byref(p)),
+              "batched plan")
+        return Plan(self, p, list(As), task, count=len(As))
+
+    def multiply_batched(self, As, task: str = "AA", stream=None) -> BatchResult:
+        p = self.plan_batched(As, task, stream)
+        try:
+            C = p.execute(stream=stream)
+            ro, no = p.offsets()
+            return BatchResult(C, ro, no)
+        finally:
+            p.close()
+
+    def get_config(self) -> dict:
+        c = SpgConfig()
+        check(lib().spg_get_config(self._h, ctypes.byref(c)), "get_config")
+        return {f: getattr(c, f) for f, _ in SpgConfig._fields_
+                if not f.startswith("reserved") and f != "struct_size"}
+
+    def set_config(self, **kw) -> None:
+        cur = self.get_config()
+        cur.update(kw)
+        cur.pop("device", None)
+        c = make_config(**cur)
+        check(lib().spg_set_config(self._h, ctypes.byref(c)), "set_config")
+
+    def autotune(self, A, task: str = "AA", reps: int = 3, stream=None) -> dict:
+        """Coordinate-descent search over bin thresholds, table loads, lanes per
+        row and heavy-path shapes, timed on A (a matrix or a list of matrices,
+        tuned as one batch); the best tuning stays in this engine."""
+        As = list(A) if isinstance(A, (list, tuple)) else [A]
+        arr = (SpgCsrDev * len(As))(*[M.struct() for M in As])
+        best = SpgConfig()
+        check(lib().spg_autotune(self._h, _task_id(task), len(As), arr, reps, ctypes.byref(best),
+                                 _stream_handle(stream)), "autotune")
+        return self.get_config()
 
     def transpose(self, A: CsrDevice, stream=None) -> CsrDevice:
         dev = A.rowptr.device

@@ -95,9 +95,13 @@ typedef struct spg_config {
   int32_t force_heavy;        /* 1 → send every non-empty row to the heavy path
                                  (debug oracle of the binning, as the reference
                                  did by forcing its global path)                 */
+  int32_t sym_load_pct;       /* symbolic tables sized for at most this load of
+                                 min(products, span), percent 20..90; 0 → 75     */
+  int32_t num_load_pct;       /* numeric tables sized for at most this load of
+                                 the exact row count, percent 20..90; 0 → 66     */
   int32_t reserved0;
   int64_t pool_release_bytes; /* memory-pool release threshold; 0 → keep all    */
-  int64_t reserved[6];
+  int64_t reserved[5];
 } spg_config;
 
 /* Result record of spg_run_ours: the reference's EngResult {ms, nnz, s, as, sq}
@@ -166,9 +170,41 @@ spg_status spg_plan_create(spg_ctx* ctx, spg_task task, const spg_csr_dev* A,
                            void* stream, spg_plan** plan);
 spg_status spg_plan_get_info(const spg_plan* plan, spg_plan_info* info);
 /* Numeric phase + in-row sort (+ mirror for AAtS) into caller-owned buffers:
- * C->rowptr (n+1), C->col / C->val (info.nnz_c).  Asynchronous on `stream`. */
+ * C->rowptr (n+1), C->col / C->val (info.nnz_c).  Asynchronous on `stream`.
+ * A plan fixes the structure only: a plan may be executed again after A's
+ * values (not its pattern) changed, and uses the current values. */
 spg_status spg_execute(spg_plan* plan, spg_csr_out* C, void* stream);
 spg_status spg_plan_destroy(spg_plan* plan);
+
+/* Batched plan: `count` independent square matrices, C_b = A_b·A_b (or A_b·A_bᵀ)
+ * for every b.  The instances are laid out on the device as one block-diagonal
+ * matrix, so each phase of the plan and of spg_execute runs as one launch over
+ * a binned row queue shared by all instances (no per-instance launches or host
+ * syncs).  spg_execute then writes the concatenation: instance b owns rows
+ * [row_off[b], row_off[b+1]) of C and entries [nnz_off[b], nnz_off[b+1]), with
+ * its own column indices.  A_b arrays must stay valid until execution ends. */
+spg_status spg_plan_create_batched(spg_ctx* ctx, spg_task task, int32_t count,
+                                   const spg_csr_dev* As, void* stream, spg_plan** plan);
+/* Instance offsets of a batched plan: row_off and nnz_off hold count+1 entries. */
+spg_status spg_plan_batch_offsets(const spg_plan* plan, int64_t* row_off, int64_t* nnz_off);
+
+/* CUDA graph of spg_execute for a plan and fixed output buffers: capture once,
+ * launch many times (same structure, same buffers; values of A may change). */
+typedef struct spg_graph spg_graph;
+spg_status spg_graph_capture(spg_plan* plan, spg_csr_out* C, void* stream, spg_graph** graph);
+spg_status spg_graph_launch(spg_graph* graph, void* stream);
+spg_status spg_graph_destroy(spg_graph* graph);
+
+/* Replace the tuning of a context (applies to plans created afterwards). */
+spg_status spg_set_config(spg_ctx* ctx, const spg_config* cfg);
+spg_status spg_get_config(const spg_ctx* ctx, spg_config* cfg);
+/* Autotuner: times spg_plan_create + spg_execute of `task` on A (a single
+ * matrix, or a batched set when count > 1) over candidate bin thresholds,
+ * table loads, lanes per row and heavy-path shapes (coordinate descent,
+ * median of `reps` timings each), leaves the best tuning in the context and
+ * copies it to *best.  Costs a few dozen products of A. */
+spg_status spg_autotune(spg_ctx* ctx, spg_task task, int32_t count, const spg_csr_dev* As,
+                        int32_t reps, spg_config* best, void* stream);
 
 /* plan + execute with C allocated from the context pool; C->nnz is set. */
 spg_status spg_multiply(spg_ctx* ctx, spg_task task, const spg_csr_dev* A,

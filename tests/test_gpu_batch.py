@@ -1,0 +1,157 @@
+"""Batched plans (many matrices as one block-diagonal product), CUDA-graph
+replay of the execute phase, and the autotuner — all checked bit for bit
+against the CPU oracle per instance."""
+import numpy as np
+import pytest
+
+import oracle
+from appt_spgemm_b200 import _capi, csr
+from appt_spgemm_b200._capi import SpgemmError
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+TASKS = ("AA", "AAt", "AAtS")
+
+
+@pytest.fixture(scope="module")
+def eng():
+    from appt_spgemm_b200.engine import Engine
+    e = Engine("cuda:0")
+    yield e
+    e.check_device_status()
+    e.close()
+
+
+def dev(A):
+    from appt_spgemm_b200.engine import CsrDevice
+    return CsrDevice.from_host(A, "cuda:0")
+
+
+def mixed_instances():
+    mats = [csr.laplace2d(9), csr.banded(700, 12, 0.3, 1), csr.erdos_renyi(900, 7.0, 2),
+            csr.CsrHost(0, np.zeros(1, np.int32), np.zeros(0, np.int32), np.zeros(0)),
+            csr.uniform(300, 40, 3), csr.rmat(10, 8, seed=4),
+            csr.CsrHost(1, np.array([0, 1], np.int32), np.array([0], np.int32), np.array([2.0])),
+            csr.CsrHost(5, np.zeros(6, np.int32), np.zeros(0, np.int32), np.zeros(0)),
+            csr.stencil27(6, 5)]
+    mats += csr.batch_mix(6, seed=9, n_min=200, n_max=3000)[0]
+    return mats
+
+
+def check_instances(res, mats, task):
+    torch.cuda.synchronize()
+    for b, A in enumerate(mats):
+        rp, col, val = res.instance(b)
+        orp, oci, ocx = oracle.multiply(A, task)
+        assert np.array_equal(rp.cpu().numpy(), orp), (b, task)
+        assert np.array_equal(col.cpu().numpy(), oci), (b, task)
+        assert np.array_equal(val.cpu().numpy().view(np.int64), ocx.view(np.int64)), (b, task)
+
+
+@pytest.mark.parametrize("task", TASKS)
+def test_batched_matches_each_instance(eng, task):
+    mats = mixed_instances()
+    res = eng.multiply_batched([dev(A) for A in mats], task)
+    check_instances(res, mats, task)
+
+
+def test_batched_rejects_column_outside_instance(eng):
+    A = csr.laplace2d(6)
+    B = csr.laplace2d(6)
+    B.col = B.col.copy()
+    B.col[-1] = 36  # a valid column of the block diagonal, but outside instance 1
+    with pytest.raises(SpgemmError) as e:
+        eng.multiply_batched([dev(A), dev(B)], "AA")
+    assert e.value.status == _capi.SPG_ERR_INVALID_CSR
+
+
+def test_graph_replay_of_execute(eng):
+    """Capture execute() once, replay it, and replay again after A's values
+    change (A·A reads A directly, so new values flow through the graph)."""
+    mats = csr.batch_mix(8, seed=11, n_min=500, n_max=4000)[0]
+    ds = [dev(A) for A in mats]
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        p = eng.plan_batched(ds, "AA", stream=side)
+        out = p.execute(stream=side)  # allocates the output buffers
+        g = p.capture_graph(out, side)
+        g.launch(side)
+    side.synchronize()
+    ro, no = p.offsets()
+    from appt_spgemm_b200.engine import BatchResult
+    check_instances(BatchResult(out, ro, no), mats, "AA")
+    for A, d in zip(mats, ds):
+        A.val = A.val * -0.5 + 0.25
+        d.val.copy_(torch.from_numpy(A.val))
+    torch.cuda.synchronize()
+    with torch.cuda.stream(side):
+        g.launch(side)
+    side.synchronize()
+    check_instances(BatchResult(out, ro, no), mats, "AA")
+    g.close()
+    p.close()
+
+
+@pytest.mark.parametrize("task", TASKS)
+def test_plan_reexecutes_with_new_values(eng, task):
+    """A plan fixes the structure; executing it (directly or through a graph)
+    after A's values changed uses the new values — also for A·Aᵀ, whose Aᵀ
+    values are re-derived (symmetric pattern and counting-sort paths)."""
+    from appt_spgemm_b200.engine import CsrDevice
+    for A in (csr.stencil27(8, 1), csr.rmat(11, 8, seed=6)):
+        d = dev(A)
+        side = torch.cuda.Stream()
+        with torch.cuda.stream(side):
+            p = eng.plan(d, task, stream=side)
+            out = p.execute(stream=side)
+            g = p.capture_graph(out, side)
+        side.synchronize()
+        for step in range(2):
+            A.val = np.cos(A.val * 3.0 + step)
+            d.val.copy_(torch.from_numpy(A.val))
+            torch.cuda.synchronize()
+            with torch.cuda.stream(side):
+                if step == 0:
+                    res = p.execute(stream=side)
+                else:
+                    res = g.launch(side)
+            side.synchronize()
+            rp, ci, cx = res.to_host()
+            orp, oci, ocx = oracle.multiply(A, task)
+            assert np.array_equal(ci, oci) and np.array_equal(rp, orp)
+            assert np.array_equal(cx.view(np.int64), ocx.view(np.int64)), (task, step)
+        g.close()
+        p.close()
+
+
+def test_autotune_keeps_results_exact(eng):
+    from appt_spgemm_b200.engine import Engine
+    A = csr.erdos_renyi(20000, 12.0, seed=21)
+    with Engine("cuda:0") as e:
+        cfg = e.autotune(dev(A), "AA", reps=1)
+        assert cfg["num_load_pct"] in (40, 50, 66, 80)
+        assert cfg["lanes_per_row"] in (0, 4, 8, 16, 32)
+        C = e.multiply(dev(A), "AA")
+        torch.cuda.synchronize()
+        rp, ci, cx = C.to_host()
+        orp, oci, ocx = oracle.multiply(A, "AA")
+        assert np.array_equal(rp, orp) and np.array_equal(ci, oci)
+        assert np.array_equal(cx.view(np.int64), ocx.view(np.int64))
+
+
+@pytest.mark.parametrize("knobs", [dict(num_load_pct=40, sym_load_pct=50),
+                                   dict(num_load_pct=80, sym_load_pct=90, max_smem_slots=2048),
+                                   dict(lanes_per_row=4, heavy_threads=256, window_bits=1 << 18)])
+def test_tuning_knobs_preserve_results(knobs):
+    from appt_spgemm_b200.engine import Engine
+    with Engine("cuda:0", **knobs) as e:
+        for A in (csr.rmat(12, 16, seed=2), csr.stencil27(10, 3)):
+            for task in TASKS:
+                C = e.multiply(dev(A), task)
+                torch.cuda.synchronize()
+                rp, ci, cx = C.to_host()
+                orp, oci, ocx = oracle.multiply(A, task)
+                assert np.array_equal(rp, orp) and np.array_equal(ci, oci), (knobs, task)
+                assert np.array_equal(cx.view(np.int64), ocx.view(np.int64)), (knobs, task)
