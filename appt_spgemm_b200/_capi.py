@@ -26,8 +26,12 @@ STATUS_NAMES = {
 SPG_ERR_INVALID_ARG = 1
 SPG_ERR_INVALID_CSR = 2
 SPG_ERR_OOM = 3
+SPG_ERR_CUDA = 4
+SPG_ERR_HASH_FULL = 5
+SPG_ERR_TIMEOUT = 6
 SPG_ERR_UNSUPPORTED = 7
 SPG_ERR_BUDGET = 8
+SPG_ERR_NOT_READY = 9
 SPG_ERR_IO = 10
 
 # spg_task
@@ -77,8 +81,29 @@ class SpgHostCsr(Structure):
                 ("col", POINTER(c_int32)), ("val", POINTER(c_double))]
 
 
+class SpgServerConfig(Structure):
+    _fields_ = [("struct_size", c_int32), ("workers", c_int32), ("memory_budget_bytes", c_int64),
+                ("batch_rows", c_int32), ("batch_max", c_int32), ("reserved", c_int64 * 4)]
+
+
+class SpgRequestInfo(Structure):
+    _fields_ = [("id", c_uint64), ("status", c_int32), ("task", c_int32), ("n", c_int32),
+                ("batched", c_int32), ("nnz_c", c_int64), ("products", c_int64),
+                ("reserved_bytes", c_int64), ("submit_ms", c_double), ("start_ms", c_double),
+                ("done_ms", c_double)]
+
+
+class SpgServerStats(Structure):
+    _fields_ = [("submitted", c_int64), ("completed", c_int64), ("rejected", c_int64),
+                ("failed", c_int64), ("batches", c_int64), ("products_completed", c_int64),
+                ("budget_bytes", c_int64), ("reserved_bytes", c_int64),
+                ("peak_reserved_bytes", c_int64), ("p50_ms", c_double), ("p99_ms", c_double),
+                ("max_ms", c_double), ("first_submit_ms", c_double), ("last_done_ms", c_double)]
+
+
 _ctx_p = c_void_p
 _plan_p = c_void_p
+_srv_p = c_void_p
 
 # name → (restype, argtypes); every function declared in include/spgemm_b200.h
 SIGNATURES = {
@@ -102,6 +127,14 @@ SIGNATURES = {
     "spg_graph_capture": (c_int32, [_plan_p, POINTER(SpgCsrOut), c_void_p, POINTER(c_void_p)]),
     "spg_graph_launch": (c_int32, [c_void_p, c_void_p]),
     "spg_graph_destroy": (c_int32, [c_void_p]),
+    "spg_server_create": (c_int32, [POINTER(SpgServerConfig), POINTER(_srv_p)]),
+    "spg_server_submit": (c_int32, [_srv_p, c_int32, POINTER(SpgCsrDev), POINTER(c_uint64)]),
+    "spg_server_poll": (c_int32, [_srv_p, c_uint64, POINTER(SpgRequestInfo)]),
+    "spg_server_wait": (c_int32, [_srv_p, c_uint64, c_int32, POINTER(SpgRequestInfo)]),
+    "spg_server_copy_result": (c_int32, [_srv_p, c_uint64, c_void_p, c_void_p, c_void_p]),
+    "spg_server_release": (c_int32, [_srv_p, c_uint64]),
+    "spg_server_stats_get": (c_int32, [_srv_p, POINTER(SpgServerStats)]),
+    "spg_server_destroy": (c_int32, [_srv_p]),
     "spg_set_config": (c_int32, [_ctx_p, POINTER(SpgConfig)]),
     "spg_get_config": (c_int32, [_ctx_p, POINTER(SpgConfig)]),
     "spg_autotune": (c_int32, [_ctx_p, c_int32, c_int32, POINTER(SpgCsrDev), c_int32,

@@ -354,3 +354,87 @@ def checksum(vals: torch.Tensor):
     check(lib().spg_checksum(vals.data_ptr() if vals.numel() else 0, vals.numel(),
                              ctypes.byref(s), ctypes.byref(a), ctypes.byref(q)), "checksum")
     return (s.value, a.value, q.value)
+
+
+class Server:
+    """Request server (spg_server_*): continuous batching of A·A / A·Aᵀ requests
+    with admission by a device-memory budget from the symbolic pass."""
+
+    def __init__(self, workers: int = 4, memory_budget_bytes: int = 0, batch_rows: int = 0,
+                 batch_max: int = 0, device=None):
+        if device is not None:
+            torch.cuda.set_device(torch.device(device))
+        torch.cuda.init()
+        cfg = _capi.SpgServerConfig()
+        cfg.struct_size = ctypes.sizeof(_capi.SpgServerConfig)
+        cfg.workers = workers
+        cfg.memory_budget_bytes = memory_budget_bytes
+        cfg.batch_rows = batch_rows
+        cfg.batch_max = batch_max
+        h = ctypes.c_void_p()
+        check(lib().spg_server_create(ctypes.byref(cfg), ctypes.byref(h)), "server create")
+        self._h = h
+        self._inputs = {}  # request id → input kept alive until the request is done
+
+    @staticmethod
+    def _info(i) -> dict:
+        return {f: getattr(i, f) for f, _ in _capi.SpgRequestInfo._fields_}
+
+    def submit(self, A: CsrDevice, task: str = "AA") -> int:
+        s = A.struct()
+        rid = ctypes.c_uint64()
+        check(lib().spg_server_submit(self._h, _task_id(task), ctypes.byref(s), ctypes.byref(rid)),
+              "submit")
+        self._inputs[rid.value] = A
+        return rid.value
+
+    def poll(self, rid: int) -> dict:
+        i = _capi.SpgRequestInfo()
+        check(lib().spg_server_poll(self._h, rid, ctypes.byref(i)), "poll")
+        return self._info(i)
+
+    def wait(self, rid: int, timeout_ms: int = -1) -> dict:
+        i = _capi.SpgRequestInfo()
+        check(lib().spg_server_wait(self._h, rid, timeout_ms, ctypes.byref(i)), "wait")
+        self._inputs.pop(rid, None)
+        return self._info(i)
+
+    def result(self, rid: int, device=None) -> CsrResult:
+        """Copy a finished result into new device tensors (the server keeps its copy)."""
+        info = self.wait(rid)
+        if info["status"] != _capi.SPG_OK:
+            raise _capi.SpgemmError(info["status"], f"request {rid} did not complete")
+        dev = torch.device(device) if device is not None else torch.device("cuda")
+        n, nnz = info["n"], info["nnz_c"]
+        rp = torch.empty(n + 1, dtype=torch.int64, device=dev)
+        col = torch.empty(max(nnz, 1), dtype=torch.int32, device=dev)
+        val = torch.empty(max(nnz, 1), dtype=torch.float64, device=dev)
+        check(lib().spg_server_copy_result(self._h, rid, rp.data_ptr(), col.data_ptr(),
+                                           val.data_ptr()), "copy result")
+        return CsrResult(n, nnz, rp, col[:nnz], val[:nnz])
+
+    def release(self, rid: int) -> None:
+        check(lib().spg_server_release(self._h, rid), "release")
+
+    def stats(self) -> dict:
+        st = _capi.SpgServerStats()
+        check(lib().spg_server_stats_get(self._h, ctypes.byref(st)), "stats")
+        return {f: getattr(st, f) for f, _ in _capi.SpgServerStats._fields_}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().spg_server_destroy(self._h)
+            self._h = None
+            self._inputs.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -206,6 +206,68 @@ spg_status spg_get_config(const spg_ctx* ctx, spg_config* cfg);
 spg_status spg_autotune(spg_ctx* ctx, spg_task task, int32_t count, const spg_csr_dev* As,
                         int32_t reps, spg_config* best, void* stream);
 
+/* ---- serving ---------------------------------------------------------------
+ * A request loop for A·A / A·Aᵀ requests of different sizes.  Worker threads,
+ * each with its own stream and engine context, take queued requests as they
+ * arrive; several requests are in flight on the device at once.  Requests on
+ * small matrices (n < batch_rows) that are queued together with the same task
+ * are merged into one batched plan (continuous batching).  Admission: after the
+ * symbolic pass gives a request's exact output size, its output plus plan
+ * workspace is reserved against the memory budget; a request waits until
+ * enough is free (results released), and a request larger than the whole budget
+ * is rejected with SPG_ERR_BUDGET.  Inputs and results stay on the device. */
+typedef struct spg_server spg_server;
+typedef struct spg_server_config {
+  int32_t struct_size;
+  int32_t workers;             /* requests (or merged batches) in flight; 0 → 4   */
+  int64_t memory_budget_bytes; /* device memory reserved at once; 0 → 150 GB     */
+  int32_t batch_rows;          /* n below which requests may be merged; 0 → 65536 */
+  int32_t batch_max;           /* requests per merged batch; 0 → 64              */
+  int64_t reserved[4];
+} spg_server_config;
+
+typedef struct spg_request_info {
+  uint64_t id;
+  int32_t status;              /* SPG_OK done, SPG_ERR_NOT_READY queued/running,
+                                  SPG_ERR_BUDGET rejected, other: failed        */
+  int32_t task;
+  int32_t n;
+  int32_t batched;             /* 1 when it ran inside a merged batch           */
+  int64_t nnz_c;
+  int64_t products;            /* intermediate products; for a request run in a
+                                  merged batch, the batch's products split by
+                                  the request's share of the output            */
+  int64_t reserved_bytes;
+  double submit_ms;            /* host clock, ms since the server started       */
+  double start_ms;
+  double done_ms;              /* the GPU finished this request's product        */
+} spg_request_info;
+
+typedef struct spg_server_stats {
+  int64_t submitted, completed, rejected, failed, batches;
+  int64_t products_completed;
+  int64_t budget_bytes, reserved_bytes, peak_reserved_bytes;
+  double p50_ms, p99_ms, max_ms;   /* latency submit → done of completed requests */
+  double first_submit_ms, last_done_ms;
+} spg_server_stats;
+
+spg_status spg_server_create(const spg_server_config* cfg, spg_server** out);
+/* Queue a request on a device CSR that stays valid until the request is done. */
+spg_status spg_server_submit(spg_server* s, spg_task task, const spg_csr_dev* A, uint64_t* id);
+spg_status spg_server_poll(spg_server* s, uint64_t id, spg_request_info* info);
+/* Wait until the request is done, rejected or failed; SPG_ERR_TIMEOUT after
+ * timeout_ms (negative: no limit). */
+spg_status spg_server_wait(spg_server* s, uint64_t id, int32_t timeout_ms, spg_request_info* info);
+/* Copy a finished result into caller buffers (device or host): rowptr n+1
+ * int64, col/val nnz_c.  The server keeps the result until released. */
+spg_status spg_server_copy_result(spg_server* s, uint64_t id, int64_t* rowptr, int32_t* col,
+                                  double* val);
+/* Drop a finished result: frees its device memory and returns its budget. */
+spg_status spg_server_release(spg_server* s, uint64_t id);
+spg_status spg_server_stats_get(spg_server* s, spg_server_stats* st);
+/* Waits for in-flight requests, frees all results, stops the workers. */
+spg_status spg_server_destroy(spg_server* s);
+
 /* plan + execute with C allocated from the context pool; C->nnz is set. */
 spg_status spg_multiply(spg_ctx* ctx, spg_task task, const spg_csr_dev* A,
                         spg_csr_out* C, void* stream);

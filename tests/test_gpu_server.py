@@ -1,0 +1,79 @@
+"""The request server: every result equals its standalone product (and the
+oracle) bit for bit while requests of different sizes run concurrently and
+small ones are merged into batches; the memory budget rejects what can never
+fit and holds back what does not fit yet."""
+import numpy as np
+import pytest
+
+import oracle
+from appt_spgemm_b200 import _capi, csr
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def dev(A):
+    from appt_spgemm_b200.engine import CsrDevice
+    return CsrDevice.from_host(A, "cuda:0")
+
+
+def request_mix():
+    mats = [csr.laplace2d(20), csr.uniform(800, 6, 1), csr.banded(3000, 9, 0.3, 2),
+            csr.erdos_renyi(2000, 8.0, 3), csr.stencil27(30, 4), csr.rmat(13, 16, seed=5),
+            csr.laplace2d(300), csr.banded(1500, 30, 0.3, 6)]
+    mats += csr.batch_mix(10, seed=7, n_min=300, n_max=5000)[0]
+    tasks = ["AA" if i % 2 == 0 else ("AAt" if i % 4 == 1 else "AAtS") for i in range(len(mats))]
+    return mats, tasks
+
+
+def test_server_results_equal_standalone_and_oracle():
+    from appt_spgemm_b200.engine import Engine, Server
+    mats, tasks = request_mix()
+    ds = [dev(A) for A in mats]
+    with Server(workers=3, batch_rows=8192, batch_max=8) as srv:
+        ids = [srv.submit(d, t) for d, t in zip(ds, tasks)]
+        infos = [srv.wait(i, timeout_ms=120000) for i in ids]
+        assert all(inf["status"] == _capi.SPG_OK for inf in infos)
+        st = srv.stats()
+        assert st["completed"] == len(mats) and st["rejected"] == 0
+        assert st["batches"] >= 1 and any(inf["batched"] for inf in infos)
+        assert st["p99_ms"] >= st["p50_ms"] > 0
+        with Engine("cuda:0") as eng:
+            for i, (A, d, t, rid) in enumerate(zip(mats, ds, tasks, ids)):
+                got = srv.result(rid)
+                alone = eng.multiply(d, t)
+                torch.cuda.synchronize()
+                g, a = got.to_host(), alone.to_host()
+                o = oracle.multiply(A, t)
+                for x, y, z in zip(g, a, o):
+                    assert np.array_equal(x.view(np.uint8), y.view(np.uint8)), (i, t)
+                    assert np.array_equal(x.view(np.uint8), np.ascontiguousarray(z).view(np.uint8))
+                srv.release(rid)
+        assert srv.stats()["reserved_bytes"] == 0
+
+
+def test_server_budget_rejects_and_holds_back():
+    from appt_spgemm_b200.engine import Server
+    big = csr.stencil27(40, 8)            # output ~ 14 MB
+    small = csr.laplace2d(30)             # output ~ 28 KB
+    out_big = 8 * (big.n + 1) + 12 * len(oracle.multiply(big, "AA")[1])
+    # a budget below the big request's output: it is rejected, the small one runs
+    with Server(workers=2, memory_budget_bytes=out_big // 2, batch_rows=1) as srv:
+        rb = srv.submit(dev(big), "AA")
+        rs = srv.submit(dev(small), "AA")
+        assert srv.wait(rb, 60000)["status"] == _capi.SPG_ERR_BUDGET
+        assert srv.wait(rs, 60000)["status"] == _capi.SPG_OK
+        assert srv.stats()["rejected"] == 1
+    # a budget that holds one big result at a time: the second waits for a release
+    with Server(workers=2, memory_budget_bytes=int(out_big * 1.6), batch_rows=1) as srv:
+        d = dev(big)
+        r1 = srv.submit(d, "AA")
+        assert srv.wait(r1, 60000)["status"] == _capi.SPG_OK
+        r2 = srv.submit(d, "AA")
+        with pytest.raises(_capi.SpgemmError) as e:
+            srv.wait(r2, timeout_ms=1500)
+        assert e.value.status == _capi.SPG_ERR_TIMEOUT
+        srv.release(r1)
+        assert srv.wait(r2, 60000)["status"] == _capi.SPG_OK
+        assert srv.stats()["peak_reserved_bytes"] <= int(out_big * 1.6)
