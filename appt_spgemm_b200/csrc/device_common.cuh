@@ -220,6 +220,92 @@ __device__ __forceinline__ void warp_bitonic_sort(U (&r)[E]) {
   }
 }
 
+// ---- stable LSD radix sort of 32-bit words in shared memory --------------------
+template <int NW>
+__device__ __forceinline__ void nw_sync() {
+  if (NW == 1) __syncwarp();
+  else __syncthreads();
+}
+
+// Sorts w[0..m) by the bit field [lo_bit, lo_bit + nbits) with DBITS-bit digits
+// (5 to 8),
+// least significant first, ping-ponging with tmp[0..m); returns the array
+// that holds the result (w or tmp).  Bits outside the field travel with the
+// word.  NW warps take part (NW = 1: the calling warp; NW > 1: the whole CTA
+// of NW warps).  Per pass warp w owns the contiguous slice [w·S, w·S + S)
+// (S = ⌈m/NW⌉ rounded up to 32): it counts its digits into cnt[d·NW + w],
+// one exclusive scan over cnt (digit-major, so warp 0's 5s precede warp 1's
+// 5s) gives every (digit, warp) its first output position, and each warp then
+// scatters its slice 32 words at a time, ranking lanes with equal digits by
+// __match_any_sync so equal digits keep their input order.  Each pass is
+// therefore stable, and for distinct fields the result is ascending in the
+// field.  cnt holds 2^DBITS·NW ints; scratch 33 ints (used when NW > 1).
+template <int NW, int DBITS>
+__device__ uint32_t* radix_sort_words(uint32_t* w, uint32_t* tmp, int m, int lo_bit, int nbits,
+                                      int* cnt, int* scratch) {
+  static_assert(DBITS >= 5 && DBITS <= 8, "digit width");
+  constexpr int R = 1 << DBITS, PER = R / 32;  // counters owned by each thread
+  constexpr uint32_t DM = R - 1;
+  const int lane = threadIdx.x & 31;
+  const int wid = NW == 1 ? 0 : (int)(threadIdx.x >> 5);
+  const int tid = NW == 1 ? lane : (int)threadIdx.x;
+  const int S = ((m + NW - 1) / NW + 31) & ~31;
+  const int s0 = min(m, wid * S), s1 = min(m, s0 + S);
+  uint32_t* src = w;
+  uint32_t* dst = tmp;
+  for (int sh = lo_bit; sh < lo_bit + nbits; sh += DBITS) {
+#pragma unroll
+    for (int k = 0; k < PER; ++k) cnt[tid * PER + k] = 0;
+    nw_sync<NW>();
+    for (int i = s0 + lane; i < s1; i += 32) atomicAdd(&cnt[((src[i] >> sh) & DM) * NW + wid], 1);
+    nw_sync<NW>();
+    int v[PER], sum = 0;
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      v[k] = cnt[tid * PER + k];
+      sum += v[k];
+    }
+    int ex;
+    if (NW == 1) {
+      int incl = sum;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      ex = incl - sum;
+    } else {
+      int tot;
+      ex = block_exclusive_scan(sum, scratch, &tot);
+    }
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      cnt[tid * PER + k] = ex;
+      ex += v[k];
+    }
+    nw_sync<NW>();
+    for (int c = s0; c < s1; c += 32) {
+      const int i = c + lane;
+      const bool on = i < s1;
+      const uint32_t x = on ? src[i] : 0u;
+      const int d = on ? (int)((x >> sh) & DM) : R;
+      const unsigned peers = __match_any_sync(0xffffffffu, d);
+      const int rank = __popc(peers & lanemask_lt());
+      const int slot = on ? d * NW + wid : 0;
+      const int base = on ? cnt[slot] : 0;
+      __syncwarp();
+      if (on && rank == 0) cnt[slot] = base + __popc(peers);
+      __syncwarp();
+      if (on) dst[base + rank] = x;
+    }
+    nw_sync<NW>();
+    uint32_t* t = src;
+    src = dst;
+    dst = t;
+  }
+  return src;
+}
+
 __host__ __device__ __forceinline__ int next_pow2_int(int x) {
   int p = 1;
   while (p < x) p <<= 1;

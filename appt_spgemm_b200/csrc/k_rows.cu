@@ -15,6 +15,7 @@
 //  - the row is compacted and bitonic-sorted in shared memory and written to
 //    its final CSR slots, so no global sort exists.
 #include <climits>
+#include <type_traits>
 
 #include "kernels.h"
 
@@ -24,6 +25,40 @@ __host__ __device__ constexpr size_t row_group_bytes(int T, int G, bool numeric)
   return numeric ? (size_t)T * 12 + (size_t)G * 16 : (size_t)T * 4 + (size_t)G * 8;
 }
 constexpr size_t kCtaScratchBytes = 256;  // 32 long longs for block reductions
+
+// Numeric CTA rows of 4096- and 8192-slot tables sort packed words with the
+// CTA-wide radix sort; its second buffer (T words) and digit counters (256
+// per warp, T/512 warps) follow the scratch.  16384-slot tables keep the
+// bitonic pair sort (the extra buffers would not fit beside the table).
+template <int LOG2T, bool NUMERIC>
+__host__ __device__ constexpr bool cta_radix() {
+  return NUMERIC && LOG2T >= 12 && LOG2T <= 13;
+}
+template <int LOG2T, bool NUMERIC>
+__host__ __device__ constexpr size_t cta_radix_bytes() {
+  return cta_radix<LOG2T, NUMERIC>() ? ((size_t)4 << LOG2T) + ((size_t)4 << LOG2T) / 2 : 0;
+}
+
+// Packs the occupied slots of keys[0..T) as ((key − lo) << LOG2T) | slot and
+// moves them to the front in slot order (in place; the values stay in their
+// slots).  Returns their count.
+template <int LOG2T>
+__device__ __forceinline__ int cta_compact_packed(int* keys, int lo, void* scratch) {
+  constexpr int T = 1 << LOG2T;
+  int m = 0;
+  for (int base = 0; base < T; base += blockDim.x) {
+    const int s = base + threadIdx.x;
+    const int key = s < T ? keys[s] : kEmptyKey;
+    const bool occ = key != kEmptyKey;
+    int tot;
+    const int ex = block_exclusive_scan(occ ? 1 : 0, (int*)scratch, &tot);
+    // writes land below base + blockDim.x; the next chunk reads only above
+    if (occ) keys[m + ex] = (int)(((uint32_t)(key - lo) << LOG2T) | (uint32_t)s);
+    m += tot;
+  }
+  __syncthreads();
+  return m;
+}
 
 __device__ __forceinline__ int grp_sum(const WarpGroup& g, int v, void*) { return g.sum(v); }
 __device__ __forceinline__ int grp_sum(const CtaGroup&, int v, void* scratch) {
@@ -81,7 +116,8 @@ __device__ __forceinline__ int grp_compact(const CtaGroup& g, int* keys, double*
 template <int LOG2T, bool NUMERIC, bool GRAM, class Grp>
 __device__ __forceinline__ void hash_row(const Grp& g, const RowArgs& a, const int row,
                                          int* __restrict__ keys, double* __restrict__ vals,
-                                         int* st_bs, int* st_len, double* st_a, void* scratch) {
+                                         int* st_bs, int* st_len, double* st_a, void* scratch,
+                                         uint32_t* rtmp, int* rcnt) {
   constexpr int T = 1 << LOG2T;
   for (int s = g.lane; s < T; s += g.G) {
     keys[s] = kEmptyKey;
@@ -131,6 +167,24 @@ __device__ __forceinline__ void hash_row(const Grp& g, const RowArgs& a, const i
     }
     g.sync();
     return;
+  }
+
+  if constexpr (cta_radix<LOG2T, NUMERIC>() && std::is_same<Grp, CtaGroup>::value) {
+    const int lo = a.lo[row];
+    if ((int64_t)a.hi[row] - lo < ((int64_t)1 << (32 - LOG2T))) {
+      int m = cta_compact_packed<LOG2T>(keys, lo, scratch);
+      const int32_t low = GRAM ? a.low_in[row] : 0;
+      const int expect = a.cnt_in[row] - low;
+      if (m != expect) {
+        if (g.lane == 0) report(a.status, DEV_ERR_OVERFLOW);
+        if (m > expect) m = expect;
+      }
+      const uint32_t* sorted = radix_sort_words<(T >> 9), 8>(
+          (uint32_t*)keys, rtmp, m, LOG2T, span_bits(lo, a.hi[row]), rcnt, (int*)scratch);
+      emit_packed<LOG2T, GRAM>(a, row, lo, m, sorted, vals, a.rowptr[row] + low, g.lane, g.G);
+      g.sync();  // the table is reused by the next row
+      return;
+    }
   }
 
   int m = grp_compact<T>(g, keys, vals, scratch);
@@ -187,7 +241,8 @@ __global__ void __launch_bounds__(256) k_hash_warp(RowArgs a) {
   }
   st_len = st_bs + a.G;
   for (int r = blockIdx.x * rows_per_cta + gi; r < a.nrows; r += gridDim.x * rows_per_cta)
-    hash_row<LOG2T, NUMERIC, GRAM>(g, a, a.rows[r], keys, vals, st_bs, st_len, st_a, nullptr);
+    hash_row<LOG2T, NUMERIC, GRAM>(g, a, a.rows[r], keys, vals, st_bs, st_len, st_a, nullptr,
+                                   nullptr, nullptr);
 }
 
 template <int LOG2T, bool NUMERIC, bool GRAM>
@@ -206,14 +261,18 @@ __global__ void __launch_bounds__(1024) k_hash_cta(RowArgs a) {
   int* st_bs = (int*)p;
   int* st_len = st_bs + G;
   void* scratch = (void*)(p + (size_t)G * 8);
+  uint32_t* rtmp = (uint32_t*)(p + (size_t)G * 8 + kCtaScratchBytes);
+  int* rcnt = (int*)(rtmp + T);
   for (int r = blockIdx.x; r < a.nrows; r += gridDim.x)
-    hash_row<LOG2T, NUMERIC, GRAM>(g, a, a.rows[r], keys, vals, st_bs, st_len, st_a, scratch);
+    hash_row<LOG2T, NUMERIC, GRAM>(g, a, a.rows[r], keys, vals, st_bs, st_len, st_a, scratch,
+                                   rtmp, rcnt);
 }
 
 int hash_bin_lanes(int bin, int lanes_cfg) {
   const int lg = bin + kMinTableLog2 - 1;
   const int T = 1 << lg;
-  if (lg >= 11) return T / 16;  // one row per CTA: 128 … 1024 threads
+  if (lg == 11) return 32;      // warp per row (k_rows_w32.cu)
+  if (lg >= 12) return T / 16;  // one row per CTA: 256 … 1024 threads
   int G = lanes_cfg > T / 8 ? lanes_cfg : T / 8;
   if (G > 32) G = 32;
   if (G > T) G = T;
@@ -246,7 +305,8 @@ static cudaError_t launch_lg(const RowArgs& a, int num_sms, cudaStream_t s) {
   constexpr int T = 1 << LOG2T;
   if (LOG2T >= 11) {
     const int threads = T / 16;
-    const size_t smem = row_group_bytes(T, threads, NUMERIC) + kCtaScratchBytes;
+    const size_t smem = row_group_bytes(T, threads, NUMERIC) + kCtaScratchBytes +
+                        cta_radix_bytes<LOG2T, NUMERIC>();
     return launch_kernel(k_hash_cta<LOG2T, NUMERIC, GRAM>, threads, smem, a.nrows, num_sms, a, s);
   }
   const int G = a.G;
@@ -286,7 +346,7 @@ cudaError_t launch_hash_bin(int bin, bool numeric, bool gram, const RowArgs& a, 
                             cudaStream_t s) {
   if (a.nrows <= 0) return cudaSuccess;
   const int lg = bin + kMinTableLog2 - 1;
-  if (a.G == 32 && lg >= 6 && lg <= 10) return launch_hash_w32(lg, numeric, gram, a, num_sms, s);
+  if (a.G == 32 && lg >= 6 && lg <= 11) return launch_hash_w32(lg, numeric, gram, a, num_sms, s);
   if (numeric) return gram ? launch_mode<true, true>(bin, a, num_sms, s)
                            : launch_mode<true, false>(bin, a, num_sms, s);
   return gram ? launch_mode<false, true>(bin, a, num_sms, s)

@@ -1,5 +1,6 @@
 // Warp-per-row shared-memory hash kernels (32 lanes per row, tables of 64 to
-// 1024 slots): the path almost every row of banded / FEM-like matrices takes.
+// 2048 slots): the path almost every row of banded / FEM-like matrices and of
+// sparse random graphs takes.
 //
 // Per row the warp
 //  - holds up to 32 entries of A's row in registers (k, a_ik, B-row bounds)
@@ -12,9 +13,13 @@
 //    no value array is cleared per row);
 //  - packs each occupied slot as ((col − lo) << log2T) | slot, sorts the
 //    packed words with a register bitonic network (E words per lane), and
-//    writes columns and the gathered values to the row's CSR slots.
-// Rows whose column span does not fit the packing, or with more than 256
-// entries, take the shared-memory pair sort instead.
+//    writes columns and the gathered values to the row's CSR slots; rows of
+//    more than 256 entries (tables of 512 slots and up) sort the packed words
+//    with a stable LSD radix sort over the column bits instead, O(m) per
+//    digit rather than the bitonic network's O(m log² m), in the table's own
+//    free space.
+// Rows whose column span does not fit the packing take the shared-memory
+// pair sort.
 #include <climits>
 
 #include "kernels.h"
@@ -50,8 +55,13 @@ __device__ __forceinline__ void insert_acc(int* keys, double* vals, int j, doubl
   }
 }
 
-// Sorted write-out through packed keys; returns false when P needs more
-// registers than supported (caller falls back to the shared pair sort).
+// Shared memory of one warp's row: the table's values (numeric) and keys.
+template <int LOG2T, bool NUMERIC>
+__host__ __device__ constexpr size_t w32_warp_bytes() {
+  return NUMERIC ? ((size_t)12 << LOG2T) : ((size_t)4 << LOG2T);
+}
+
+// Sorted write-out through packed keys held E per lane in registers.
 template <int E, int LOG2T, bool GRAM>
 __device__ __forceinline__ void sort_write(const RowArgs& a, int row, int lo, int m, int* keys,
                                           const double* vals, int64_t base) {
@@ -90,24 +100,7 @@ __device__ __forceinline__ void sort_write(const RowArgs& a, int row, int lo, in
     kw[0] = r[0];
   }
   __syncwarp();
-  const int cb = a.colbase ? a.colbase[row] : 0;
-  for (int e = lane; e < m; e += 32) {
-    const uint32_t pk = (uint32_t)keys[e];
-    const int j = lo + (int)(pk >> LOG2T);
-    const double v = vals[pk & ((1u << LOG2T) - 1u)];
-    a.ccol[base + e] = j - cb;
-    a.cval[base + e] = v;
-    if (GRAM && j > row) {
-      const int pos = atomicAdd(&a.cursor[j], 1);
-      if (pos < a.low_in[j]) {
-        const int64_t d = a.lowptr[j] + pos;
-        a.lcol[d] = row - cb;
-        a.lval[d] = v;
-      } else {
-        report(a.status, DEV_ERR_OVERFLOW);
-      }
-    }
-  }
+  emit_packed<LOG2T, GRAM>(a, row, lo, m, (const uint32_t*)keys, vals, base, lane, 32);
 }
 
 // Fallback: compact (key, value) pairs in slot order and bitonic-sort them in
@@ -164,7 +157,11 @@ __global__ void __launch_bounds__(256, 5) k_hash_w32(RowArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   constexpr int T = 1 << LOG2T;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  unsigned char* base_p = smem + (size_t)w * (NUMERIC ? (size_t)T * 12 : (size_t)T * 4);
+  // rows of more than 256 entries (tables of 512 slots and up) take the radix
+  // sort, with DBITS-bit digits whose counters fit the table's free tail
+  constexpr bool RADIX = NUMERIC && LOG2T >= 9;
+  constexpr int DBITS = LOG2T == 9 ? 7 : 8;
+  unsigned char* base_p = smem + (size_t)w * w32_warp_bytes<LOG2T, NUMERIC>();
   double* vals = (double*)base_p;
   int* keys = (int*)(base_p + (NUMERIC ? (size_t)T * 8 : 0));
 
@@ -287,26 +284,45 @@ __global__ void __launch_bounds__(256, 5) k_hash_w32(RowArgs a) {
     const int64_t base = a.rowptr[row] + low;
     const int lo = a.lo[row];
     const bool packs = (int64_t)a.hi[row] - lo < ((int64_t)1 << (32 - LOG2T));
-    if (!packs || expect > 256) {
+    // Radix rows compact (packed word, value) pairs to the front of keys /
+    // vals; the sort's second buffer (m words) then lives in vals[m..T) and
+    // its 2^DBITS counters in keys[m..T), which needs 3m <= 2T and
+    // m + 2^DBITS <= T (true up to a 66% table load).
+    const bool radix = RADIX && packs && expect > 256 && 3 * expect <= 2 * T &&
+                       expect + (1 << DBITS) <= T;
+    if (!packs || (expect > 256 && !radix)) {
       pair_sort_write<LOG2T, GRAM>(a, row, keys, vals, base, expect);
       __syncwarp();
       continue;
     }
-    // compact occupied slots as packed words, in place
+    // compact occupied slots as packed words ((col − lo) << LOG2T | index of
+    // the value: its slot, or for radix rows its compacted position), in place
     int m = 0;
     for (int c = 0; c < T; c += 32) {
       const int s = c + lane;
       const int key = keys[s];
+      const double v = radix ? vals[s] : 0.0;
       const bool occ = key != kEmptyKey;
       const unsigned bal = __ballot_sync(kFull, occ);
       const int pos = m + __popc(bal & lanemask_lt());
       __syncwarp();
-      if (occ) keys[pos] = (int)(((uint32_t)(key - lo) << LOG2T) | (uint32_t)s);
+      if (occ) {
+        keys[pos] = (int)(((uint32_t)(key - lo) << LOG2T) | (uint32_t)(radix ? pos : s));
+        if (radix) vals[pos] = v;
+      }
       m += __popc(bal);
       __syncwarp();
     }
     if (m != expect && lane == 0) report(a.status, DEV_ERR_OVERFLOW);
     if (m > expect) m = expect;
+    if (radix) {
+      const uint32_t* sorted = radix_sort_words<1, DBITS>(
+          (uint32_t*)keys, (uint32_t*)(vals + m), m, LOG2T, span_bits(lo, a.hi[row]), keys + m,
+          nullptr);
+      emit_packed<LOG2T, GRAM>(a, row, lo, m, sorted, vals, base, lane, 32);
+      __syncwarp();
+      continue;
+    }
     const int P = next_pow2_int(m);
     if (P <= 32) sort_write<1, LOG2T, GRAM>(a, row, lo, m, keys, vals, base);
     else if (P <= 64) sort_write<2, LOG2T, GRAM>(a, row, lo, m, keys, vals, base);
@@ -318,9 +334,8 @@ __global__ void __launch_bounds__(256, 5) k_hash_w32(RowArgs a) {
 
 template <int LOG2T, bool NUMERIC, bool GRAM>
 static cudaError_t launch_w32(const RowArgs& a, int num_sms, cudaStream_t s) {
-  constexpr int T = 1 << LOG2T;
   auto kernel = k_hash_w32<LOG2T, NUMERIC, GRAM>;
-  const size_t per = NUMERIC ? (size_t)T * 12 : (size_t)T * 4;
+  const size_t per = w32_warp_bytes<LOG2T, NUMERIC>();
   int rows = 8;  // warps (rows) per CTA
   while (rows > 1 && per * rows > 64 * 1024) rows >>= 1;
   const size_t smem = per * rows;
@@ -352,6 +367,7 @@ static cudaError_t w32_mode(int log2t, const RowArgs& a, int num_sms, cudaStream
     case 8: return launch_w32<8, NUMERIC, GRAM>(a, num_sms, s);
     case 9: return launch_w32<9, NUMERIC, GRAM>(a, num_sms, s);
     case 10: return launch_w32<10, NUMERIC, GRAM>(a, num_sms, s);
+    case 11: return launch_w32<11, NUMERIC, GRAM>(a, num_sms, s);
   }
   return cudaErrorNotSupported;
 }

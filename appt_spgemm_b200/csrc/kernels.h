@@ -118,6 +118,40 @@ struct RowArgs {
   const int32_t* colbase;
 };
 
+// Writes m sorted packed words ((col − lo) << LOG2T | slot) as a row's columns
+// and the values of their table slots, lanes first, first + stride, … (so the
+// stores are coalesced); the Gram path also mirrors each entry above the
+// diagonal into the lower store through the column's atomic cursor.
+template <int LOG2T, bool GRAM>
+__device__ __forceinline__ void emit_packed(const RowArgs& a, int row, int lo, int m,
+                                            const uint32_t* sorted, const double* vals,
+                                            int64_t base, int first, int stride) {
+  const int cb = a.colbase ? a.colbase[row] : 0;
+  for (int e = first; e < m; e += stride) {
+    const uint32_t pk = sorted[e];
+    const int j = lo + (int)(pk >> LOG2T);
+    const double v = vals[pk & ((1u << LOG2T) - 1u)];
+    a.ccol[base + e] = j - cb;
+    a.cval[base + e] = v;
+    if (GRAM && j > row) {
+      const int pos = atomicAdd(&a.cursor[j], 1);
+      if (pos < a.low_in[j]) {
+        const int64_t d = a.lowptr[j] + pos;
+        a.lcol[d] = row - cb;
+        a.lval[d] = v;
+      } else {
+        report(a.status, DEV_ERR_OVERFLOW);
+      }
+    }
+  }
+}
+
+// Number of bits needed for the column field of a row spanning [lo, hi].
+__device__ __forceinline__ int span_bits(int lo, int hi) {
+  const uint32_t span = (uint32_t)(hi - lo);
+  return span ? 32 - __clz((int)span) : 0;
+}
+
 // Warp-per-row kernels (k_rows_w32.cu) for table bins of up to 1024 slots
 // with 32 lanes per row; returns cudaErrorNotSupported for other bins.
 cudaError_t launch_hash_w32(int log2t, bool numeric, bool gram, const RowArgs& a, int num_sms,

@@ -432,13 +432,26 @@ def run_serve(args):
                 done = []
 
                 def consumer():
-                    for k in range(nreq):
-                        while ids[k] is None:
-                            time.sleep(0.0005)
-                        info = srv.wait(ids[k])
-                        done.append((k, info))
-                        if info["status"] == _capi.SPG_OK:
-                            srv.release(ids[k])
+                    # release results in completion order: a request waiting
+                    # for budget may need the memory of later ones
+                    pending = set()
+                    nxt = 0
+                    while len(done) < nreq:
+                        while nxt < nreq and ids[nxt] is not None:
+                            pending.add(nxt)
+                            nxt += 1
+                        finished = []
+                        for k in pending:
+                            info = srv.poll(ids[k])
+                            if info["status"] != _capi.SPG_ERR_NOT_READY:
+                                finished.append((k, info))
+                        for k, info in finished:
+                            pending.discard(k)
+                            done.append((k, info))
+                            if info["status"] == _capi.SPG_OK:
+                                srv.release(ids[k])
+                        if not finished:
+                            time.sleep(0.0002)
 
                 th = threading.Thread(target=consumer)
                 th.start()

@@ -147,7 +147,8 @@ def test_autotune_keeps_results_exact(eng):
 def test_tuning_knobs_preserve_results(knobs):
     from appt_spgemm_b200.engine import Engine
     with Engine("cuda:0", **knobs) as e:
-        for A in (csr.rmat(12, 16, seed=2), csr.stencil27(10, 3)):
+        for A in (csr.rmat(12, 16, seed=2), csr.stencil27(10, 3),
+                  csr.erdos_renyi(20000, 25.0, seed=4)):
             for task in TASKS:
                 C = e.multiply(dev(A), task)
                 torch.cuda.synchronize()

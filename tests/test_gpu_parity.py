@@ -73,6 +73,15 @@ def test_every_bin(eng, per_row, task):
     run_case(eng, csr.uniform(n, per_row, seed=per_row), task, f"uniform{per_row}")
 
 
+# rows of roughly 300 to 5000 entries spread over 70,000 columns: the radix
+# sorts of the 512/1024-slot warp tables and of the 2048- to 8192-slot CTA
+# tables, with three 8-bit digit passes over 17-bit column fields
+@pytest.mark.parametrize("deg", [18.0, 30.0, 60.0])
+@pytest.mark.parametrize("task", TASKS)
+def test_wide_rows_three_digit_passes(eng, deg, task):
+    run_case(eng, csr.erdos_renyi(70000, deg, seed=int(deg)), task, f"er70k_d{int(deg)}")
+
+
 @pytest.mark.parametrize("lanes", [4, 8, 16, 32])
 def test_lanes_per_row(lanes):
     from appt_spgemm_b200.engine import Engine
