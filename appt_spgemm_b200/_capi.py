@@ -52,7 +52,7 @@ class SpgConfig(Structure):
     _fields_ = [("struct_size", c_int32), ("device", c_int32), ("lanes_per_row", c_int32),
                 ("max_smem_slots", c_int32), ("heavy_threads", c_int32),
                 ("window_bits", c_int32), ("force_heavy", c_int32), ("sym_load_pct", c_int32),
-                ("num_load_pct", c_int32), ("reserved0", c_int32),
+                ("num_load_pct", c_int32), ("heavy_split", c_int32),
                 ("pool_release_bytes", c_int64), ("reserved", c_int64 * 5)]
 
 

@@ -62,6 +62,31 @@ __device__ __forceinline__ int hash_insert(int* keys, int j, uint32_t* status) {
   return -1;
 }
 
+// CAS-first linear probe: one shared atomic per probe, the loop exits on an
+// empty slot (claimed) or on the key itself.  In the numeric phase the value
+// is then 0.0 + v for a freshly claimed slot and slot + v otherwise — a
+// select, not a branch — so no value array is cleared between rows.
+template <int LOG2T, bool NUMERIC>
+__device__ __forceinline__ void insert_acc(int* keys, double* vals, int j, double v,
+                                           uint32_t* status) {
+  constexpr unsigned T = 1u << LOG2T;
+  unsigned h = hash_slot<LOG2T>(j);
+  int old = atomicCAS(keys + h, kEmptyKey, j);
+  unsigned probe = 1;
+  while (old != kEmptyKey && old != j) {
+    if (probe++ == T) {
+      report(status, DEV_ERR_HASH_FULL);
+      return;
+    }
+    h = (h + 1) & (T - 1);
+    old = atomicCAS(keys + h, kEmptyKey, j);
+  }
+  if (NUMERIC) {
+    const double cur = vals[h];
+    vals[h] = __dadd_rn(old == kEmptyKey ? 0.0 : cur, v);
+  }
+}
+
 // ---- lane groups -------------------------------------------------------------
 // A row is processed by a group of G lanes: a power-of-two slice of one warp
 // (G <= 32, several rows per CTA) or the whole CTA (G = blockDim.x > 32).

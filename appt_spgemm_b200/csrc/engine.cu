@@ -136,6 +136,13 @@ struct spg_plan {
   // derived values (block-diagonal copy, Aᵀ) still match A: true right after
   // planning; every later execute recomputes them from A's current values
   bool values_fresh = true;
+  // heavy rows: per-block distinct-column counts from the symbolic phase
+  // (nullptr when their number exceeds kMaxHeavyBlocks: the numeric phase
+  // then takes the CTA dense-window kernel) and the windowed kernel's cursors
+  int64_t* blk_off = nullptr;
+  uint16_t* blk_cnt = nullptr;
+  int blk_log2 = 12;
+  int4* hcur = nullptr;
 };
 
 struct spg_graph {
@@ -208,6 +215,33 @@ spg_config merged_config(const spg_config* user) {
       c.lanes_per_row != 16 && c.lanes_per_row != 32)
     c.lanes_per_row = 0;
   return c;
+}
+
+constexpr int64_t kMaxHeavyBlocks = (int64_t)1 << 30;  // 2 GB of block counts
+constexpr int64_t kHeavySplitDefault = 128;           // mean B-row length
+
+// Smallest exact row count that the numeric binning sends to the heavy path
+// (table of more than 2^num_lg slots at num_load percent).
+int64_t numeric_heavy_min(int num_lg, int num_load) {
+  int64_t l = 1, h = (int64_t)1 << 40;
+  while (l < h) {
+    const int64_t mid = (l + h) / 2;
+    int lg = ceil_log2_64(mid * 100 / num_load + 1);
+    if (lg < kMinTableLog2) lg = kMinTableLog2;
+    if (lg > num_lg) h = mid; else l = mid + 1;
+  }
+  return l;
+}
+
+// Windows of the heavy numeric kernel: at most this many distinct columns,
+// within its table's load limit and the radix sort's room (3m <= 2T,
+// m + 256 <= T); blocks above it are cut into windows of 2^sub_log2 columns.
+int heavy_cap(int num_load) {
+  const int T = 1 << kHeavyTableLog2;
+  int cap = (int)((int64_t)T * num_load / 100);
+  cap = std::min(cap, 2 * T / 3);
+  cap = std::min(cap, T - 256);
+  return std::max(cap, 32);
 }
 
 int table_log2_cap(int slots) {
@@ -345,21 +379,40 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
   TRY(palloc(p, &counts, 4 * kNumBins));
   TRY(palloc(p, &rows_sym, n));
   const int force = ctx->cfg.force_heavy ? 1 : 0;
+  const int num_lg = table_log2_cap(ctx->cfg.max_smem_slots);
   BinSource bsym{0, n, p->f, p->lo, p->hi, nullptr, nullptr, kMaxTableLog2, force,
-                 ctx->cfg.sym_load_pct};
+                 ctx->cfg.sym_load_pct,
+                 numeric_heavy_min(num_lg, ctx->cfg.num_load_pct)};
   {
     ProfScope ps(ctx, "plan/bin_sym", st);
     TRY_CUDA(launch_bin_rows(bsym, hist, counts, rows_sym, st), "symbolic binning");
   }
+  // column blocks of the heavy rows (4096 columns, or 1024 when the symbolic
+  // window is not a multiple of 4096)
+  p->blk_log2 = ctx->cfg.window_bits % 4096 == 0 ? 12 : 10;
+  {
+    int32_t* nblk;
+    void* btmp;
+    TRY(palloc(p, &nblk, n));
+    TRY(palloc(p, &p->blk_off, (int64_t)n + 1));
+    TRY(palloc(p, (char**)&btmp, (int64_t)scan_tmp_bytes(n)));
+    ProfScope ps(ctx, "plan/heavy_blocks", st);
+    TRY_CUDA(launch_heavy_blocks(bsym, p->blk_log2, nblk, p->blk_off, btmp, st), "heavy blocks");
+  }
   int64_t* hp = p->ctx->h_pin;
   TRY_CUDA(cudaMemcpyAsync(hp, counts, sizeof(int64_t) * 2 * kNumBins, cudaMemcpyDeviceToHost, st),
            "bin readback");
+  TRY_CUDA(cudaMemcpyAsync(hp + 2 * kNumBins, p->blk_off + n, sizeof(int64_t),
+                           cudaMemcpyDeviceToHost, st), "bin readback");
   TRY_CUDA(cudaStreamSynchronize(st), "bin sync");
   int64_t sym_count[kNumBins], sym_start[kNumBins];
   for (int b = 0; b < kNumBins; ++b) {
     sym_count[b] = hp[b];
     sym_start[b] = hp[kNumBins + b];
   }
+  const int64_t total_blocks = hp[2 * kNumBins];
+  if (total_blocks > 0 && total_blocks <= kMaxHeavyBlocks)
+    TRY(palloc(p, &p->blk_cnt, total_blocks));
 
   // symbolic phase
   TRY(palloc(p, &p->rownnz, n));
@@ -396,6 +449,9 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
     h.lo = p->lo;
     h.hi = p->hi;
     h.window_bits = ctx->cfg.window_bits;
+    h.blk_off = p->blk_off;
+    h.blk_cnt = p->blk_cnt;
+    h.blk_log2 = p->blk_log2;
     ProfScope ps(ctx, "sym/heavy", st);
     TRY_CUDA(launch_heavy(false, gram, h, ctx->cfg.heavy_threads, ctx->num_sms, st),
              "symbolic heavy");
@@ -418,7 +474,6 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
 
   // numeric binning by exact counts, stats; host sync #3 (nnz(C))
   TRY(palloc(p, &p->rows_num, n));
-  const int num_lg = table_log2_cap(ctx->cfg.max_smem_slots);
   BinSource bnum{1, n, p->f, p->lo, p->hi, p->rownnz, gram ? p->rowlow : nullptr, num_lg, force,
                  ctx->cfg.num_load_pct};
   {
@@ -455,6 +510,7 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
   p->info.max_row_products = (int64_t)sv[1];
   p->info.max_row_nnz = (int64_t)sv[2];
   p->info.heavy_rows = p->num_count[kHeavyBin];
+  if (p->num_count[kHeavyBin] > 0 && p->blk_cnt) TRY(palloc(p, &p->hcur, Ad->nnz));
   for (int b = 1; b < kNumBins; ++b)
     if (p->num_count[b] > 0) ++bins_used;
   p->info.bins_used = bins_used;
@@ -550,8 +606,27 @@ spg_status execute_impl(spg_plan* p, spg_csr_out* C, cudaStream_t st) {
       h.lo = p->lo;
       h.hi = p->hi;
       h.window_bits = ctx->cfg.window_bits;
+      h.blk_off = p->blk_off;
+      h.blk_cnt = p->blk_cnt;
+      h.blk_log2 = p->blk_log2;
+      h.cap = heavy_cap(ctx->cfg.num_load_pct);
+      h.sub_log2 = 31 - __builtin_clz((unsigned)h.cap);  // largest power of two <= cap
+      if (h.sub_log2 > p->blk_log2) h.sub_log2 = p->blk_log2;
+      h.hcur = p->hcur;
+      // rows whose B rows are short on average (mean length below heavy_split)
+      // stream through the warp kernel's windows; rows fed by long B rows, or
+      // all rows without block counts, take the CTA kernel, whose 1024
+      // threads share each long B row and whose per-k barrier is paid once
+      // per row rather than once per window
+      const bool windows = p->blk_cnt && p->hcur;
+      h.f = p->f;
+      h.split = !windows ? 0
+                : ctx->cfg.heavy_split > 0 ? (int64_t)ctx->cfg.heavy_split : kHeavySplitDefault;
       ProfScope ps(ctx, "num/heavy", st);
-      cudaError_t e = launch_heavy(true, gram, h, ctx->cfg.heavy_threads, ctx->num_sms, st);
+      cudaError_t e = cudaSuccess;
+      if (windows) e = launch_heavy_w32(gram, h, ctx->num_sms, st);
+      if (e == cudaSuccess)
+        e = launch_heavy(true, gram, h, ctx->cfg.heavy_threads, ctx->num_sms, st);
       if (e != cudaSuccess) { result = cuda_status(e, "numeric heavy"); break; }
     }
     if (gram && p->nnz_low > 0) {
@@ -966,6 +1041,7 @@ spg_status spg_autotune(spg_ctx* ctx, spg_task task, int32_t count, const spg_cs
       {&spg_config::max_smem_slots, {2048, 4096, 8192, 16384}, false},
       {&spg_config::heavy_threads, {256, 512, 1024}, true},
       {&spg_config::window_bits, {1 << 18, 1 << 19, 1 << 20}, true},
+      {&spg_config::heavy_split, {1, 32, 128, 512, 1 << 30}, true},
   };
   for (const Knob& k : knobs) {
     if (k.heavy_only && !has_heavy) continue;

@@ -14,6 +14,8 @@
 // In the reference every row above 767 products went to a per-row global hash
 // arena of next_pow2(4f/3+1) slots (src/spgemm_engine.cuh:51-57, :79, :101)
 // followed by the global radix sort.
+#include <algorithm>
+
 #include "kernels.h"
 
 namespace spg {
@@ -78,14 +80,27 @@ __global__ void __launch_bounds__(1024) k_heavy_sym(HeavyArgs h) {
       for (int i = threadIdx.x; i < nwords; i += blockDim.x) bm[i] = 0u;
       __syncthreads();
       mark_window(a, row, w0, nwords, bm, st_bs, st_ex, scratch);
+      // a warp per column block of the window (32 or more words): the bit
+      // counts are the row totals and, when asked for, the block counts
       int lc = 0, lcl = 0;
-      for (int i = threadIdx.x; i < nwords; i += blockDim.x) {
-        const uint32_t wd = bm[i];
-        lc += __popc(wd);
-        if (GRAM) {
-          const long long c0 = w0 + 32LL * i;
-          if (c0 + 32 <= row) lcl += __popc(wd);
-          else if (c0 < row) lcl += __popc(wd & ((1u << (unsigned)(row - c0)) - 1u));
+      const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+      const int wpb = 1 << (h.blk_log2 - 5);
+      const long long blk0 = (w0 - lo) >> h.blk_log2;
+      for (int blk = wid; blk * wpb < nwords; blk += nwarps) {
+        int bc = 0;
+        for (int i = blk * wpb + lane; i < min((blk + 1) * wpb, nwords); i += 32) {
+          const uint32_t wd = bm[i];
+          bc += __popc(wd);
+          if (GRAM) {
+            const long long c0 = w0 + 32LL * i;
+            if (c0 + 32 <= row) lcl += __popc(wd);
+            else if (c0 < row) lcl += __popc(wd & ((1u << (unsigned)(row - c0)) - 1u));
+          }
+        }
+        lc += bc;
+        if (h.blk_cnt) {
+          for (int o = 16; o > 0; o >>= 1) bc += __shfl_xor_sync(0xffffffffu, bc, o);
+          if (lane == 0) h.blk_cnt[h.blk_off[row] + blk0 + blk] = (uint16_t)min(bc, 65535);
         }
       }
       c += block_sum64(lc, (long long*)scratch);
@@ -127,6 +142,7 @@ __global__ void __launch_bounds__(1024) k_heavy_num(HeavyArgs h) {
     const int lo = GRAM ? max(h.lo[row], row) : h.lo[row];
     const int32_t low = GRAM ? a.low_in[row] : 0;
     const long long expect = (long long)a.cnt_in[row] - low;
+    if (heavy_row_windowed(h, row)) continue;  // the windowed warp kernel's row
     const int64_t base = a.rowptr[row] + low;
     const int cb = a.colbase ? a.colbase[row] : 0;
     long long written = 0;
@@ -254,6 +270,26 @@ static cudaError_t launch_h(K kernel, int threads, size_t smem, const HeavyArgs&
   kernel<<<(unsigned)grid, threads, smem, s>>>(h);
   SPG_COUNT_LAUNCH();
   return cudaGetLastError();
+}
+
+__global__ void k_heavy_blocks(BinSource bsym, int blk_log2, int32_t* __restrict__ nblk) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < bsym.n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    nblk[i] = row_bin(bsym, (int)i) == kHeavyBin
+                  ? (int32_t)((((int64_t)bsym.hi[i] - bsym.lo[i]) >> blk_log2) + 1)
+                  : 0;
+}
+
+cudaError_t launch_heavy_blocks(const BinSource& bsym, int blk_log2, int32_t* nblk,
+                                int64_t* blk_off, void* scan_tmp, cudaStream_t s) {
+  if (bsym.n > 0) {
+    const int64_t blocks = std::min<int64_t>(((int64_t)bsym.n + 255) / 256, 4096);
+    k_heavy_blocks<<<(unsigned)blocks, 256, 0, s>>>(bsym, blk_log2, nblk);
+    SPG_COUNT_LAUNCH();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return launch_scan_i32_i64(nblk, blk_off, bsym.n, scan_tmp, s);
 }
 
 cudaError_t launch_heavy(bool numeric, bool gram, const HeavyArgs& h, int threads, int num_sms,

@@ -30,31 +30,6 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 
-// CAS-first linear probe: one shared atomic per probe, the loop exits on an
-// empty slot (claimed) or on the key itself.  In the numeric phase the value
-// is then 0.0 + v for a freshly claimed slot and slot + v otherwise — a
-// select, not a branch — so no value array is cleared between rows.
-template <int LOG2T, bool NUMERIC>
-__device__ __forceinline__ void insert_acc(int* keys, double* vals, int j, double v,
-                                           uint32_t* status) {
-  constexpr unsigned T = 1u << LOG2T;
-  unsigned h = hash_slot<LOG2T>(j);
-  int old = atomicCAS(keys + h, kEmptyKey, j);
-  unsigned probe = 1;
-  while (old != kEmptyKey && old != j) {
-    if (probe++ == T) {
-      report(status, DEV_ERR_HASH_FULL);
-      return;
-    }
-    h = (h + 1) & (T - 1);
-    old = atomicCAS(keys + h, kEmptyKey, j);
-  }
-  if (NUMERIC) {
-    const double cur = vals[h];
-    vals[h] = __dadd_rn(old == kEmptyKey ? 0.0 : cur, v);
-  }
-}
-
 // Shared memory of one warp's row: the table's values (numeric) and keys.
 template <int LOG2T, bool NUMERIC>
 __host__ __device__ constexpr size_t w32_warp_bytes() {

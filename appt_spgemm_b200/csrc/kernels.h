@@ -39,6 +39,10 @@ struct BinSource {
   int max_log2;             // largest shared table (log2 slots) before the heavy path
   int force_heavy;
   int load_pct;             // table sized for at most this load (percent)
+  // symbolic: rows with min(products, span) >= heavy_min also go heavy, so
+  // every row the numeric binning sends to the heavy path has block counts
+  // from the heavy symbolic kernel (0: no such rule)
+  int64_t heavy_min;
 };
 
 __host__ __device__ __forceinline__ int ceil_log2_64(int64_t x) {
@@ -65,6 +69,7 @@ __host__ __device__ __forceinline__ int row_bin(const BinSource& s, int i) {
   }
   const int64_t want = size * 100 / s.load_pct + 1;
   if (s.force_heavy) return kHeavyBin;
+  if (s.mode == 0 && s.heavy_min > 0 && size >= s.heavy_min) return kHeavyBin;
   int lg = ceil_log2_64(want);
   if (lg < kMinTableLog2) lg = kMinTableLog2;
   if (lg > s.max_log2) return kHeavyBin;
@@ -152,7 +157,7 @@ __device__ __forceinline__ int span_bits(int lo, int hi) {
   return span ? 32 - __clz((int)span) : 0;
 }
 
-// Warp-per-row kernels (k_rows_w32.cu) for table bins of up to 1024 slots
+// Warp-per-row kernels (k_rows_w32.cu) for table bins of up to 2048 slots
 // with 32 lanes per row; returns cudaErrorNotSupported for other bins.
 cudaError_t launch_hash_w32(int log2t, bool numeric, bool gram, const RowArgs& a, int num_sms,
                             cudaStream_t s);
@@ -170,10 +175,41 @@ struct HeavyArgs {
   const int32_t* lo;        // output column span per row
   const int32_t* hi;
   int32_t window_bits;      // W (multiple of 32 * threads)
+  // column blocks: heavy row i's span [lo, hi] is cut into blocks of
+  // 2^blk_log2 columns from lo; blk_cnt[blk_off[i] + b] is the number of
+  // distinct output columns in block b (saturated at 65535), written by the
+  // symbolic kernel when blk_cnt is set and read by the windowed numeric one
+  const int64_t* blk_off;   // per row (n + 1), 0 blocks for rows not heavy
+  uint16_t* blk_cnt;
+  int32_t blk_log2;
+  int32_t cap;              // numeric: most distinct columns per window
+  int32_t sub_log2;         // numeric: window width inside a block above cap
+  int4* hcur;               // numeric: per entry of A {B cursor, B row end, next column, 0}
+  // numeric: rows whose mean B-row length f / nnz(A row) is below `split`
+  // take the windowed warp kernel, the others the CTA kernel (each kernel
+  // skips the other's rows); split 0 sends every row to the CTA kernel
+  int64_t split;
+  const int64_t* f;         // products per row (pre-pass)
 };
+
+// Row r of the heavy list goes to the windowed warp kernel.
+__device__ __forceinline__ bool heavy_row_windowed(const HeavyArgs& h, int row) {
+  const int64_t len = (int64_t)h.r.A.rowptr[row + 1] - h.r.A.rowptr[row];
+  return h.split > 0 && h.f[row] < h.split * len;
+}
 cudaError_t launch_heavy(bool numeric, bool gram, const HeavyArgs& a, int threads, int num_sms,
                          cudaStream_t s);
 size_t heavy_smem_bytes(bool numeric, int threads, int window_bits);
+
+// Blocks per row for the heavy rows of `bsym` (0 for the others), scanned into
+// blk_off[0..n] (launch_scan_i32_i64 with tmp of scan_tmp_bytes(n)).
+cudaError_t launch_heavy_blocks(const BinSource& bsym, int blk_log2, int32_t* nblk,
+                                int64_t* blk_off, void* scan_tmp, cudaStream_t s);
+
+// Windowed numeric phase of heavy rows (k_heavy_w32.cu): a warp per row walks
+// the row's column blocks in windows of at most `cap` distinct columns.
+cudaError_t launch_heavy_w32(bool gram, const HeavyArgs& a, int num_sms, cudaStream_t s);
+constexpr int kHeavyTableLog2 = 11;  // its shared table: 2048 slots per warp
 
 // ---- transpose and segment sort (k_transpose.cu) ----------------------------
 

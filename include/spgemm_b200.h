@@ -99,7 +99,10 @@ typedef struct spg_config {
                                  min(products, span), percent 20..90; 0 → 75     */
   int32_t num_load_pct;       /* numeric tables sized for at most this load of
                                  the exact row count, percent 20..90; 0 → 66     */
-  int32_t reserved0;
+  int32_t heavy_split;        /* heavy rows whose B rows average fewer entries
+                                 than this take the warp-per-row windowed
+                                 kernel, the others the CTA-per-row kernel
+                                 (1: all CTA); 0 → 128                          */
   int64_t pool_release_bytes; /* memory-pool release threshold; 0 → keep all    */
   int64_t reserved[5];
 } spg_config;

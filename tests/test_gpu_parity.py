@@ -90,13 +90,16 @@ def test_lanes_per_row(lanes):
             run_case(e, csr.erdos_renyi(3000, 9.0, seed=lanes), task, f"er/lanes{lanes}")
 
 
-@pytest.mark.parametrize("window", [0, 4096])
-def test_force_heavy_dense_windows(window):
-    """Every row through the CTA-per-row dense-window path (the reference's
-    debugging trick of forcing all rows onto its global path), with one window
-    and with many windows per row."""
+@pytest.mark.parametrize("window,split", [(0, 1 << 30), (4096, 1 << 30), (3072, 1 << 30),
+                                          (0, 1), (4096, 1), (0, 0)])
+def test_force_heavy_dense_windows(window, split):
+    """Every row through the heavy path (the reference's debugging trick of
+    forcing all rows onto its global path): symbolic bitmap windows of 2^20,
+    4096 and 3072 columns (the last cuts rows into 1024-column blocks instead
+    of 4096); numeric rows all through the windowed warp kernel (split 2^30),
+    all through the CTA kernel (split 1) or divided by the default rule."""
     from appt_spgemm_b200.engine import Engine
-    with Engine("cuda:0", force_heavy=1, window_bits=window) as e:
+    with Engine("cuda:0", force_heavy=1, window_bits=window, heavy_split=split) as e:
         for A, lab in ((csr.laplace2d(40), "lap40"), (csr.rmat(11, 8, seed=2), "rmat11"),
                        (csr.erdos_renyi(20000, 4.0, seed=3), "er20k")):
             for task in TASKS:
@@ -106,6 +109,16 @@ def test_force_heavy_dense_windows(window):
 @pytest.mark.parametrize("task", TASKS)
 def test_rmat_heavy_rows(eng, task):
     run_case(eng, csr.rmat(13, 16, seed=3), task, "rmat13")
+
+
+@pytest.mark.parametrize("split", [1, 1 << 30])
+@pytest.mark.parametrize("task", TASKS)
+def test_rmat_heavy_split(split, task):
+    """R-MAT heavy rows all through the CTA kernel (split 1) or all through
+    the windowed warp kernel (split 2^30), dense blocks included."""
+    from appt_spgemm_b200.engine import Engine
+    with Engine("cuda:0", heavy_split=split) as e:
+        run_case(e, csr.rmat(14, 16, seed=4), task, f"rmat14/split{split}")
 
 
 @pytest.mark.parametrize("task", TASKS)
