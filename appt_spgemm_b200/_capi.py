@@ -53,7 +53,8 @@ class SpgConfig(Structure):
                 ("max_smem_slots", c_int32), ("heavy_threads", c_int32),
                 ("window_bits", c_int32), ("force_heavy", c_int32), ("sym_load_pct", c_int32),
                 ("num_load_pct", c_int32), ("heavy_split", c_int32),
-                ("pool_release_bytes", c_int64), ("reserved", c_int64 * 5)]
+                ("pool_release_bytes", c_int64), ("heavy_block_budget", c_int64),
+                ("reserved", c_int64 * 4)]
 
 
 class SpgEngResult(Structure):

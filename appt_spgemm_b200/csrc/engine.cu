@@ -137,7 +137,7 @@ struct spg_plan {
   // planning; every later execute recomputes them from A's current values
   bool values_fresh = true;
   // heavy rows: per-block distinct-column counts from the symbolic phase
-  // (nullptr when their number exceeds kMaxHeavyBlocks: the numeric phase
+  // (nullptr when their number exceeds heavy_block_budget: the numeric phase
   // then takes the CTA dense-window kernel) and the windowed kernel's cursors
   int64_t* blk_off = nullptr;
   uint16_t* blk_cnt = nullptr;
@@ -214,11 +214,11 @@ spg_config merged_config(const spg_config* user) {
   if (c.lanes_per_row != 0 && c.lanes_per_row != 4 && c.lanes_per_row != 8 &&
       c.lanes_per_row != 16 && c.lanes_per_row != 32)
     c.lanes_per_row = 0;
+  if (c.heavy_block_budget <= 0) c.heavy_block_budget = (int64_t)1 << 27;  // 256 MB of counts
   return c;
 }
 
-constexpr int64_t kMaxHeavyBlocks = (int64_t)1 << 30;  // 2 GB of block counts
-constexpr int64_t kHeavySplitDefault = 128;           // mean B-row length
+constexpr int64_t kHeavySplitDefault = 128;  // mean B-row length
 
 // Smallest exact row count that the numeric binning sends to the heavy path
 // (table of more than 2^num_lg slots at num_load percent).
@@ -387,15 +387,17 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
     ProfScope ps(ctx, "plan/bin_sym", st);
     TRY_CUDA(launch_bin_rows(bsym, hist, counts, rows_sym, st), "symbolic binning");
   }
-  // column blocks of the heavy rows (4096 columns, or 1024 when the symbolic
-  // window is not a multiple of 4096)
-  p->blk_log2 = ctx->cfg.window_bits % 4096 == 0 ? 12 : 10;
+  // column blocks of the heavy rows: 1024 columns, so that a block never
+  // holds more distinct columns than a window (cap >= 1024 at the default
+  // load) and windows are packed from the counts alone; wider when that many
+  // counts would exceed kHeavyBlockBudget (chosen after the readback below)
+  p->blk_log2 = 10;
+  int32_t* nblk;
+  void* btmp;
+  TRY(palloc(p, &nblk, n));
+  TRY(palloc(p, &p->blk_off, (int64_t)n + 1));
+  TRY(palloc(p, (char**)&btmp, (int64_t)scan_tmp_bytes(n)));
   {
-    int32_t* nblk;
-    void* btmp;
-    TRY(palloc(p, &nblk, n));
-    TRY(palloc(p, &p->blk_off, (int64_t)n + 1));
-    TRY(palloc(p, (char**)&btmp, (int64_t)scan_tmp_bytes(n)));
     ProfScope ps(ctx, "plan/heavy_blocks", st);
     TRY_CUDA(launch_heavy_blocks(bsym, p->blk_log2, nblk, p->blk_off, btmp, st), "heavy blocks");
   }
@@ -410,9 +412,21 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
     sym_count[b] = hp[b];
     sym_start[b] = hp[kNumBins + b];
   }
-  const int64_t total_blocks = hp[2 * kNumBins];
-  if (total_blocks > 0 && total_blocks <= kMaxHeavyBlocks)
-    TRY(palloc(p, &p->blk_cnt, total_blocks));
+  // Σ over heavy rows of ((hi − lo) >> b) + 1 is at most
+  // total_1024 / 2^(b−10) + rows, so the wider blocks need no second readback
+  int64_t total_blocks = hp[2 * kNumBins];
+  const int64_t heavy_sym = sym_count[kHeavyBin];
+  const int64_t budget = ctx->cfg.heavy_block_budget;
+  while (total_blocks > budget && p->blk_log2 < 20 &&
+         ctx->cfg.window_bits % (2 << p->blk_log2) == 0) {
+    ++p->blk_log2;
+    total_blocks = (hp[2 * kNumBins] >> (p->blk_log2 - 10)) + heavy_sym;
+  }
+  if (p->blk_log2 > 10) {
+    ProfScope ps(ctx, "plan/heavy_blocks", st);
+    TRY_CUDA(launch_heavy_blocks(bsym, p->blk_log2, nblk, p->blk_off, btmp, st), "heavy blocks");
+  }
+  if (total_blocks > 0 && total_blocks <= budget) TRY(palloc(p, &p->blk_cnt, total_blocks));
 
   // symbolic phase
   TRY(palloc(p, &p->rownnz, n));
@@ -613,11 +627,9 @@ spg_status execute_impl(spg_plan* p, spg_csr_out* C, cudaStream_t st) {
       h.sub_log2 = 31 - __builtin_clz((unsigned)h.cap);  // largest power of two <= cap
       if (h.sub_log2 > p->blk_log2) h.sub_log2 = p->blk_log2;
       h.hcur = p->hcur;
-      // rows whose B rows are short on average (mean length below heavy_split)
-      // stream through the warp kernel's windows; rows fed by long B rows, or
-      // all rows without block counts, take the CTA kernel, whose 1024
-      // threads share each long B row and whose per-k barrier is paid once
-      // per row rather than once per window
+      // rows fed by many short B rows stream through the warp kernel's
+      // windows; rows dominated by long B rows, rows of more than 2^17
+      // products, or all rows without block counts take the CTA kernel
       const bool windows = p->blk_cnt && p->hcur;
       h.f = p->f;
       h.split = !windows ? 0

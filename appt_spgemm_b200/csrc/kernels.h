@@ -185,17 +185,22 @@ struct HeavyArgs {
   int32_t cap;              // numeric: most distinct columns per window
   int32_t sub_log2;         // numeric: window width inside a block above cap
   int4* hcur;               // numeric: per entry of A {B cursor, B row end, next column, 0}
-  // numeric: rows whose mean B-row length f / nnz(A row) is below `split`
-  // take the windowed warp kernel, the others the CTA kernel (each kernel
-  // skips the other's rows); split 0 sends every row to the CTA kernel
+  // numeric: rows fed by many short B rows (mean length below `split`) take
+  // the windowed warp kernel, rows dominated by long B rows the CTA kernel,
+  // whose 1024 threads stream each long B row (each kernel skips the other's
+  // rows); split 0: all to the CTA kernel
   int64_t split;
   const int64_t* f;         // products per row (pre-pass)
 };
 
-// Row r of the heavy list goes to the windowed warp kernel.
+// The heavy row goes to the windowed warp kernel: mean B-row length
+// f / nnz(A row) below split, and at most kWarpRowMaxProducts products (one
+// warp walks its row alone: a larger row would set the kernel's tail).
+constexpr int64_t kWarpRowMaxProducts = (int64_t)1 << 17;
 __device__ __forceinline__ bool heavy_row_windowed(const HeavyArgs& h, int row) {
+  if (h.split <= 0 || h.f[row] > kWarpRowMaxProducts) return false;
   const int64_t len = (int64_t)h.r.A.rowptr[row + 1] - h.r.A.rowptr[row];
-  return h.split > 0 && h.f[row] < h.split * len;
+  return h.f[row] < h.split * len;
 }
 cudaError_t launch_heavy(bool numeric, bool gram, const HeavyArgs& a, int threads, int num_sms,
                          cudaStream_t s);

@@ -6,7 +6,8 @@ through the public API with host buffers.
 
 Workload: the 3-D 27-point stencil on a 96³ grid (n = 884,736, nnz = 23.4M,
 values uniform(−1,1) from a seed), structurally symmetric, numerically
-unsymmetric; one step = one A·A plus one A·Aᵀ (the engine's Gram path).
+unsymmetric; one step = one A·A plus one A·Aᵀ (through Aᵀ; the Gram path,
+which gives the same C, is timed per call beside the line).
 Inputs (284 MB) and outputs (2 × 1.3 GB) exceed the 126 MB L2, so no flush
 is needed between steps.
 
@@ -43,15 +44,19 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--side", type=int, default=SIDE, help="stencil grid side (96 = the benchmark)")
-    ap.add_argument("--aat-task", default="AAtS", choices=["AAt", "AAtS"],
-                    help="engine task used for A·Aᵀ")
+    ap.add_argument("--aat-task", default="AAt", choices=["AAt", "AAtS"],
+                    help="engine task used for A·Aᵀ (AAt: the product through Aᵀ, the faster "
+                         "path on this matrix; AAtS: the Gram path, upper triangle + mirror, "
+                         "also timed beside the line)")
     ap.add_argument("--no-baselines", action="store_true",
                     help="skip the CPU oracle, cuSPARSE and reference-GPU baselines")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="CPU work of the oracle baseline sample")
-    ap.add_argument("--mode", choices=["plain", "batch", "serve"], default="plain",
-                    help="plain: the headline stencil benchmark; batch: 512 matrices in one "
-                         "batched product vs back-to-back calls; serve: Poisson request stream")
+    ap.add_argument("--mode", choices=["plain", "rmat", "batch", "serve"], default="plain",
+                    help="plain: the headline stencil benchmark; rmat: the power-law graph "
+                         "(R-MAT 2^20, heavy rows); batch: 512 matrices in one batched product "
+                         "vs back-to-back calls; serve: Poisson request stream")
+    ap.add_argument("--rmat-scale", type=int, default=20, help="R-MAT scale of --mode rmat")
     ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--serve-requests", type=int, default=300,
                     help="requests per arrival rate in --mode serve")
@@ -296,6 +301,105 @@ def reference_gpu_baseline(A, p_aa, p_aat):
 
 
 # ---------------------------------------------------------------------------
+# power-law graph: R-MAT 2^20 (edge factor 16, (.57,.19,.19,.05), seed 3)
+# ---------------------------------------------------------------------------
+def run_rmat(args):
+    import torch
+
+    from appt_spgemm_b200 import csr
+    from appt_spgemm_b200.engine import CsrDevice, Engine
+
+    t0 = time.time()
+    A = csr.rmat(args.rmat_scale, 16, seed=3)
+    gen_s = time.time() - t0
+    prods = {"AA": csr.products(A, "AA"), "AAt": csr.products(A, "AAt")}
+    n, nnz = A.n, A.nnz
+    dA = CsrDevice.from_host(A, "cuda:0")
+    eng = Engine("cuda:0")
+    stream = torch.cuda.current_stream()
+    peak, peak_kind = hbm_peak()
+    tasks = {}
+    kernels = {}
+    with ClockSampler(0) as clocks:
+        for task in ("AA", "AAt"):
+            plan = eng.plan(dA, task)
+            info = dict(plan.info)
+            plan.close()
+            for _ in range(max(args.warmup, 0)):
+                C = eng.multiply(dA, task)
+                torch.cuda.synchronize()
+                del C
+            eng.profile_reset()
+            eng.profile_enable(True)
+            ts = []
+            for _ in range(max(args.steps, 1)):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                C = eng.multiply(dA, task)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                del C
+                ts.append(e0.elapsed_time(e1))
+            eng.profile_enable(False)
+            prof = eng.profile_read()
+            ms = statistics.median(ts)
+            alg = 4 * (n + 1) + 12 * nnz + 8 * (n + 1) + 12 * info["nnz_c"]
+            tasks[task] = {"ms_median": round(ms, 3), "ms_mean": round(statistics.mean(ts), 3),
+                           "gflops": round(2.0 * prods[task] / (ms * 1e-3) / 1e9, 3),
+                           "products": prods[task], "nnz_c": info["nnz_c"],
+                           "heavy_rows": info["heavy_rows"],
+                           "alg_bytes": int(alg),
+                           "hbm_frac": round(alg / (ms * 1e-3) / 1e9 / peak, 4)}
+            kernels[task] = {k: round(v["ms"] / len(ts), 3) for k, v in
+                             sorted(prof["kernels"].items(), key=lambda kv: -kv[1]["ms"])[:8]}
+            launches = int(prof.get("launches", 0))
+    total_ms = tasks["AA"]["ms_median"] + tasks["AAt"]["ms_median"]
+    value = 2.0 * (prods["AA"] + prods["AAt"]) / (total_ms * 1e-3) / 1e9
+    top_label, top_ms = max(kernels["AA"].items(), key=lambda kv: kv[1])
+    line = {"metric": "GFLOP/s (2×intermediate products/s) A·A & A·Aᵀ, power-law graph",
+            "value": round(value, 3), "unit": "GFLOP/s", "mode": "rmat", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total_ms, 3),
+            "higher_is_better": True, "dtype": "f64", "data": "synthetic (seeded generator)",
+            "config": {"workload": f"R-MAT scale {args.rmat_scale} (n={n}, nnz={nnz}), edge "
+                                   "factor 16, (a,b,c,d)=(.57,.19,.19,.05), seed 3, duplicates "
+                                   "merged, self-loops kept, values uniform(0,1); one step = "
+                                   "A·A + A·Aᵀ", "generation_s": round(gen_s, 1),
+                       "l2": "C exceeds L2 by far; no flush needed"},
+            "tasks": tasks, "kernels_ms_per_call": kernels,
+            "roofline": {"bound": "hbm", "kernel": "whole call (A·A)",
+                         "achieved": round(tasks["AA"]["alg_bytes"] /
+                                           (tasks["AA"]["ms_median"] * 1e-3) / 1e9, 1),
+                         "peak": peak, "unit": "GB/s", "frac": tasks["AA"]["hbm_frac"],
+                         "peak_source": peak_kind, "traffic": None,
+                         "top_kernel": top_label, "top_kernel_share": round(
+                             top_ms / tasks["AA"]["ms_median"], 3)},
+            "gpu_launches_per_call": launches // max(args.steps, 1),
+            "clocks": clocks.summary()}
+    del dA
+    eng.close()
+    torch.cuda.empty_cache()
+    if not args.no_baselines:
+        big = max(t["nnz_c"] for t in tasks.values()) >= 2**31
+        if big:
+            why = ("not run: C has more than 2^31 - 1 entries, which cusparseSpGEMM's "
+                   "32-bit CSR and the reference engine's int32 C row offsets "
+                   "(src/spgemm_engine.cuh:91) cannot index")
+            line["baselines"] = {"cusparse": {"unsupported": why},
+                                 "reference_gpu_engine": {"unsupported": why}}
+        else:
+            dA = CsrDevice.from_host(A, "cuda:0")
+            line["baselines"] = {"cusparse": cusparse_baseline(dA, A, prods["AA"], prods["AAt"]),
+                                 "reference_gpu_engine": reference_gpu_baseline(
+                                     A, prods["AA"], prods["AAt"])}
+            del dA
+        nthreads = os.cpu_count() or 1
+        gf, p, secs, sample = cpu_oracle_rate(A, args.cpu_seconds, nthreads)
+        line["cpu_baseline"] = {"value": round(gf, 3), "unit": "GFLOP/s", "cores": nthreads,
+                                "kind": "port", "sample": sample + f" ({p} products, {secs:.1f} s)"}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
 # batched products: 512 matrices, one batched plan vs back-to-back plain calls
 # ---------------------------------------------------------------------------
 def run_batch(args):
@@ -499,6 +603,9 @@ def main():
     if args.impl == "reference":
         run_reference(args)
         return
+    if args.mode == "rmat":
+        run_rmat(args)
+        return
     if args.mode == "batch":
         run_batch(args)
         return
@@ -598,6 +705,21 @@ def main():
                     "share_of_step": round(rec["ms"] / (ms * args.steps), 4)}
     call_alg = sum(4 * (n + 1) + 12 * nnz + 8 * (n + 1) + 12 * i["nnz_c"] for i in infos.values())
 
+    # per-call times of the three tasks (the Gram path gives the same C as
+    # A·Aᵀ; it is timed here beside the line, not inside the step)
+    per_task_ms = {}
+    for task in ("AA", "AAt", "AAtS"):
+        ts = []
+        for _ in range(3):
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a0.record(stream)
+            C = eng.multiply(dA, task)
+            a1.record(stream)
+            torch.cuda.synchronize()
+            del C
+            ts.append(a0.elapsed_time(a1))
+        per_task_ms[task] = round(statistics.median(ts), 4)
+
     result = {"metric": "GFLOP/s (2×intermediate products/s) A·A & A·Aᵀ",
               "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world,
               "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
@@ -613,6 +735,7 @@ def main():
               "kernels_ms_per_step": {k: round(v["ms"] / args.steps, 4)
                                       for k, v in sorted(kernels.items())},
               "products": {"AA": p_aa, "AAt": p_aat},
+              "ms_per_call": per_task_ms,
               "nnz_c": {t: i["nnz_c"] for t, i in infos.items()},
               "clocks": clocks.summary()}
 

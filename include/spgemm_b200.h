@@ -99,12 +99,17 @@ typedef struct spg_config {
                                  min(products, span), percent 20..90; 0 → 75     */
   int32_t num_load_pct;       /* numeric tables sized for at most this load of
                                  the exact row count, percent 20..90; 0 → 66     */
-  int32_t heavy_split;        /* heavy rows whose B rows average fewer entries
-                                 than this take the warp-per-row windowed
-                                 kernel, the others the CTA-per-row kernel
-                                 (1: all CTA); 0 → 128                          */
+  int32_t heavy_split;        /* heavy rows of at most 2^17 products whose B
+                                 rows average fewer entries than this take the
+                                 warp-per-row windowed kernel, the others the
+                                 CTA-per-row kernel (1: all CTA); 0 → 128      */
   int64_t pool_release_bytes; /* memory-pool release threshold; 0 → keep all    */
-  int64_t reserved[5];
+  int64_t heavy_block_budget; /* most per-block column counts kept for heavy
+                                 rows (2 bytes each; blocks widen from 1024
+                                 columns to stay within it, and without them
+                                 every heavy row takes the CTA kernel);
+                                 0 → 2^27                                       */
+  int64_t reserved[4];
 } spg_config;
 
 /* Result record of spg_run_ours: the reference's EngResult {ms, nnz, s, as, sq}

@@ -96,8 +96,9 @@ def test_force_heavy_dense_windows(window, split):
     """Every row through the heavy path (the reference's debugging trick of
     forcing all rows onto its global path): symbolic bitmap windows of 2^20,
     4096 and 3072 columns (the last cuts rows into 1024-column blocks instead
-    of 4096); numeric rows all through the windowed warp kernel (split 2^30),
-    all through the CTA kernel (split 1) or divided by the default rule."""
+    of 4096); numeric rows through the windowed warp kernel (split 2^30:
+    every row of at most 2^17 products), all through the CTA kernel (split 1)
+    or divided by the default rule."""
     from appt_spgemm_b200.engine import Engine
     with Engine("cuda:0", force_heavy=1, window_bits=window, heavy_split=split) as e:
         for A, lab in ((csr.laplace2d(40), "lap40"), (csr.rmat(11, 8, seed=2), "rmat11"),
@@ -111,11 +112,25 @@ def test_rmat_heavy_rows(eng, task):
     run_case(eng, csr.rmat(13, 16, seed=3), task, "rmat13")
 
 
+@pytest.mark.parametrize("budget", [1 << 18, 1 << 16, 1])
+def test_heavy_block_budget(budget):
+    """A small block-count budget widens the column blocks of the heavy rows
+    (30,000 rows of ~7,000 entries over 30,000 columns: 4096-column blocks at
+    2^18, one 32768-column block per row at 2^16, cut into fixed 1024-column
+    windows); a budget below one count per row leaves no counts, and every
+    heavy row takes the CTA kernel."""
+    from appt_spgemm_b200.engine import Engine
+    A = csr.erdos_renyi(30000, 90.0, seed=6)
+    with Engine("cuda:0", heavy_block_budget=budget) as e:
+        for task in TASKS:
+            run_case(e, A, task, f"er30k/budget{budget}")
+
+
 @pytest.mark.parametrize("split", [1, 1 << 30])
 @pytest.mark.parametrize("task", TASKS)
 def test_rmat_heavy_split(split, task):
-    """R-MAT heavy rows all through the CTA kernel (split 1) or all through
-    the windowed warp kernel (split 2^30), dense blocks included."""
+    """R-MAT heavy rows of at most 2^17 products through the windowed warp
+    kernel (split 2^30) or all heavy rows through the CTA kernel (split 1)."""
     from appt_spgemm_b200.engine import Engine
     with Engine("cuda:0", heavy_split=split) as e:
         run_case(e, csr.rmat(14, 16, seed=4), task, f"rmat14/split{split}")
