@@ -74,16 +74,17 @@ static void sort_cols(int32_t* v, int64_t m) {
   }
 }
 
-/* Number of distinct columns of row i of A·B. */
-static int64_t row_count(spa_t* s, int32_t i, const int32_t* Ap, const int32_t* Ai,
-                         const int32_t* Bp, const int32_t* Bi) {
+/* Number of distinct columns of row i of A·B.  `stamp` marks the columns
+ * seen in this visit: distinct for every visit made with one accumulator. */
+static int64_t row_count(spa_t* s, int32_t i, int32_t stamp, const int32_t* Ap,
+                         const int32_t* Ai, const int32_t* Bp, const int32_t* Bi) {
   int64_t c = 0;
   for (int32_t p = Ap[i]; p < Ap[i + 1]; ++p) {
     int32_t k = Ai[p];
     for (int32_t q = Bp[k]; q < Bp[k + 1]; ++q) {
       int32_t j = Bi[q];
-      if (s->mark[j] != i) {
-        s->mark[j] = i;
+      if (s->mark[j] != stamp) {
+        s->mark[j] = stamp;
         ++c;
       }
     }
@@ -92,9 +93,9 @@ static int64_t row_count(spa_t* s, int32_t i, const int32_t* Ap, const int32_t* 
 }
 
 /* Row i of A·B: sorted columns into cols, values into vals; returns count. */
-static int64_t row_fill(spa_t* s, int32_t i, const int32_t* Ap, const int32_t* Ai,
-                        const double* Ax, const int32_t* Bp, const int32_t* Bi, const double* Bx,
-                        int32_t* cols, double* vals) {
+static int64_t row_fill(spa_t* s, int32_t i, int32_t stamp, const int32_t* Ap,
+                        const int32_t* Ai, const double* Ax, const int32_t* Bp,
+                        const int32_t* Bi, const double* Bx, int32_t* cols, double* vals) {
   int64_t m = 0;
   for (int32_t p = Ap[i]; p < Ap[i + 1]; ++p) {
     int32_t k = Ai[p];
@@ -102,8 +103,8 @@ static int64_t row_fill(spa_t* s, int32_t i, const int32_t* Ap, const int32_t* A
     for (int32_t q = Bp[k]; q < Bp[k + 1]; ++q) {
       int32_t j = Bi[q];
       double v = a * Bx[q];
-      if (s->mark[j] != i) {
-        s->mark[j] = i;
+      if (s->mark[j] != stamp) {
+        s->mark[j] = stamp;
         s->acc[j] = 0.0;
         s->list[m++] = j;
       }
@@ -136,7 +137,7 @@ int64_t oracle_count(int32_t n, const int32_t* Ap, const int32_t* Ai, const int3
 #pragma omp for schedule(dynamic, 64)
 #endif
       for (int32_t i = 0; i < n; ++i) {
-        int64_t c = row_count(&s, i, Ap, Ai, Bp, Bi);
+        int64_t c = row_count(&s, i, i, Ap, Ai, Bp, Bi);
         rownnz[i] = c;
         total += c;
       }
@@ -164,7 +165,7 @@ int oracle_fill(int32_t n, const int32_t* Ap, const int32_t* Ai, const double* A
 #pragma omp for schedule(dynamic, 64)
 #endif
       for (int32_t i = 0; i < n; ++i) {
-        int64_t m = row_fill(&s, i, Ap, Ai, Ax, Bp, Bi, Bx, Ci + Cp[i], Cx + Cp[i]);
+        int64_t m = row_fill(&s, i, i, Ap, Ai, Ax, Bp, Bi, Bx, Ci + Cp[i], Cx + Cp[i]);
         if (m != Cp[i + 1] - Cp[i]) failed = 1;
       }
     }
@@ -240,7 +241,7 @@ int64_t oracle_rows_stream(int32_t n, const int32_t* Ap, const int32_t* Ai, cons
 #pragma omp for schedule(dynamic, 16)
 #endif
       for (int32_t i = r0; i < r1; ++i) {
-        int64_t m = row_fill(&sp, i, Ap, Ai, Ax, Bp, Bi, Bx, cols, vals);
+        int64_t m = row_fill(&sp, i, i, Ap, Ai, Ax, Bp, Bi, Bx, cols, vals);
         total += m;
         for (int64_t t = 0; t < m; ++t) {
           double x = vals[t];
@@ -260,6 +261,67 @@ int64_t oracle_rows_stream(int32_t n, const int32_t* Ap, const int32_t* Ai, cons
     chk3[2] = sq;
   }
   return failed ? -1 : total;
+}
+
+/*
+ * A sample of rows of C = A·B (rows[0..m), any order, for checking products
+ * too large to hold whole): their distinct counts into rownnz[0..m); returns
+ * the total, or -1.
+ */
+int64_t oracle_rows_count(int32_t n, const int32_t* Ap, const int32_t* Ai, const int32_t* Bp,
+                          const int32_t* Bi, const int32_t* rows, int32_t m, int64_t* rownnz,
+                          int nthreads) {
+  int64_t total = 0;
+  int failed = 0;
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel reduction(+ : total) reduction(| : failed)
+#endif
+  {
+    spa_t s;
+    if (spa_init(&s, n) != 0) {
+      failed = 1;
+    } else {
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 4)
+#endif
+      for (int32_t t = 0; t < m; ++t) {
+        int64_t c = row_count(&s, rows[t], t, Ap, Ai, Bp, Bi);
+        rownnz[t] = c;
+        total += c;
+      }
+    }
+    spa_free(&s);
+  }
+  return failed ? -1 : total;
+}
+
+/* The sampled rows themselves, into Ci/Cx at offsets Cp (m+1, from the
+ * counts).  Returns 0 or -1. */
+int oracle_rows_fill(int32_t n, const int32_t* Ap, const int32_t* Ai, const double* Ax,
+                     const int32_t* Bp, const int32_t* Bi, const double* Bx, const int32_t* rows,
+                     int32_t m, const int64_t* Cp, int32_t* Ci, double* Cx, int nthreads) {
+  int failed = 0;
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel reduction(| : failed)
+#endif
+  {
+    spa_t s;
+    if (spa_init(&s, n) != 0) {
+      failed = 1;
+    } else {
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 4)
+#endif
+      for (int32_t t = 0; t < m; ++t) {
+        int64_t c = row_fill(&s, rows[t], t, Ap, Ai, Ax, Bp, Bi, Bx, Ci + Cp[t], Cx + Cp[t]);
+        if (c != Cp[t + 1] - Cp[t]) failed = 1;
+      }
+    }
+    spa_free(&s);
+  }
+  return failed ? -1 : 0;
 }
 
 int oracle_max_threads(void) {

@@ -42,6 +42,12 @@ def _load():
         L.oracle_rows_stream.restype = ctypes.c_int64
         L.oracle_rows_stream.argtypes = [ctypes.c_int32, _i32p, _i32p, _f64p, _i32p, _i32p, _f64p,
                                          ctypes.c_int32, ctypes.c_int32, ctypes.c_int, _f64p]
+        L.oracle_rows_count.restype = ctypes.c_int64
+        L.oracle_rows_count.argtypes = [ctypes.c_int32, _i32p, _i32p, _i32p, _i32p, _i32p,
+                                        ctypes.c_int32, _i64p, ctypes.c_int]
+        L.oracle_rows_fill.restype = ctypes.c_int
+        L.oracle_rows_fill.argtypes = [ctypes.c_int32, _i32p, _i32p, _f64p, _i32p, _i32p, _f64p,
+                                       _i32p, ctypes.c_int32, _i64p, _i32p, _f64p, ctypes.c_int]
         L.oracle_max_threads.restype = ctypes.c_int
         L.oracle_max_threads.argtypes = []
         _lib = L
@@ -125,6 +131,34 @@ def rows_stream(A, B, r0: int, r1: int, nthreads: int = 0):
     if m < 0:
         raise MemoryError("oracle rows_stream failed")
     return int(m), (float(chk[0]), float(chk[1]), float(chk[2]))
+
+
+def multiply_rows(A, rows, task: str = "AA", B=None, nthreads: int = 0):
+    """Rows `rows` (int array, any order) of C = A·B, B as in multiply() unless
+    given: (rowptr int64 over the sample, col int32, val float64) — the check
+    for products too large to compute whole."""
+    n, rp, col, val = _arrs(A)
+    if B is None:
+        B = _Csr(n, rp, col, val) if task == "AA" else transpose(A)
+    _, brp, bcol, bval = _arrs(B)
+    r = np.ascontiguousarray(rows, dtype=np.int32)
+    m = len(r)
+    L = _load()
+    cnt = np.zeros(max(m, 1), dtype=np.int64)
+    tot = L.oracle_rows_count(n, _p(rp, _i32p), _p(col, _i32p), _p(brp, _i32p), _p(bcol, _i32p),
+                              _p(r, _i32p), m, _p(cnt, _i64p), nthreads)
+    if tot < 0:
+        raise MemoryError("oracle rows count failed")
+    cp = np.zeros(m + 1, dtype=np.int64)
+    np.cumsum(cnt[:m], out=cp[1:])
+    ci = np.zeros(max(tot, 1), dtype=np.int32)
+    cx = np.zeros(max(tot, 1), dtype=np.float64)
+    rc = L.oracle_rows_fill(n, _p(rp, _i32p), _p(col, _i32p), _p(val, _f64p), _p(brp, _i32p),
+                            _p(bcol, _i32p), _p(bval, _f64p), _p(r, _i32p), m, _p(cp, _i64p),
+                            _p(ci, _i32p), _p(cx, _f64p), nthreads)
+    if rc != 0:
+        raise RuntimeError("oracle rows fill failed")
+    return cp, ci[:tot], cx[:tot]
 
 
 def max_threads() -> int:

@@ -117,3 +117,18 @@ def test_empty_and_tiny():
     Z = csr.CsrHost(5, np.zeros(6, np.int32), np.zeros(0, np.int32), np.zeros(0))
     cp, ci, cx = oracle.multiply(Z, "AA")
     assert list(cp) == [0] * 6
+
+
+def test_multiply_rows_matches_full_product():
+    """The row-sample oracle (used to check products too large to compute
+    whole) gives exactly the rows of the full product, in the order asked."""
+    A = csr.rmat(11, 8, seed=5)
+    rng = np.random.default_rng(3)
+    rows = rng.integers(0, A.n, 300)
+    for task in ("AA", "AAt"):
+        cp, ci, cx = oracle.multiply(A, task)
+        sp, si, sx = oracle.multiply_rows(A, rows, task)
+        for t, r in enumerate(rows):
+            a, b = slice(cp[r], cp[r + 1]), slice(sp[t], sp[t + 1])
+            assert np.array_equal(ci[a], si[b])
+            assert np.array_equal(cx[a].view(np.int64), sx[b].view(np.int64))
