@@ -596,6 +596,28 @@ def run_serve(args):
 
 
 # ---------------------------------------------------------------------------
+# replicas: every rank runs the whole workload; the job's step time is the
+# slowest rank's, its throughput the sum of the replicas' work over that time
+# ---------------------------------------------------------------------------
+def replica_step_time(ms, device):
+    """Max over ranks of this rank's step time in ms (the rank's own time
+    when no process group is running)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(ms)
+    t = torch.tensor([float(ms)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(work_per_step, ms, world):
+    """Whole-job GFLOP/s: `world` replicas, each 2·products = work_per_step
+    per step, over the slowest rank's step time."""
+    return world * work_per_step / (ms * 1e-3) / 1e9
+
+
+# ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
 def main():
@@ -657,13 +679,10 @@ def main():
         torch.cuda.synchronize()
     eng.profile_enable(False)
     prof = eng.profile_read()
-    ms = e0.elapsed_time(e1) / max(args.steps, 1)
+    ms = replica_step_time(e0.elapsed_time(e1) / max(args.steps, 1), dev)
     if world > 1:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
-    value = world * work_per_step / (ms * 1e-3) / 1e9
+    value = replica_value(work_per_step, ms, world)
 
     # per-task info, dominant kernel and its roofline
     infos = {}
