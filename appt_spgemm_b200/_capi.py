@@ -143,6 +143,7 @@ SIGNATURES = {
     "spg_profile_enable": (c_int32, [_ctx_p, c_int32]),
     "spg_profile_reset": (c_int32, [_ctx_p]),
     "spg_profile_read": (c_int32, [_ctx_p, c_char_p, c_uint64]),
+    "spg_drop_zeros": (c_int32, [_ctx_p, POINTER(SpgCsrOut), c_void_p]),
     "spg_transpose": (c_int32, [_ctx_p, POINTER(SpgCsrDev), c_void_p, c_void_p, c_void_p,
                                 c_void_p]),
     "spg_transpose_noalloc": (c_int32, [POINTER(SpgCsrDev), c_void_p, c_void_p, c_void_p,

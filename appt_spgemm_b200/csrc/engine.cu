@@ -1120,6 +1120,76 @@ spg_status spg_free(spg_ctx* ctx, void* dev_ptr, void* stream) {
   return SPG_OK;
 }
 
+spg_status spg_drop_zeros(spg_ctx* ctx, spg_csr_out* C, void* stream) {
+  begin_call();
+  if (!ctx || !C || !C->rowptr) return set_error(SPG_ERR_INVALID_ARG, "null argument");
+  if (C->n < 0 || C->nnz < 0) return set_error(SPG_ERR_INVALID_ARG, "bad output shape");
+  if (C->nnz == 0) return SPG_OK;
+  if (!C->col || !C->val) return set_error(SPG_ERR_INVALID_ARG, "null output arrays");
+  TRY_CUDA(cudaSetDevice(ctx->device), "set device");
+  const int32_t n = C->n;
+  spg_plan tmp;  // borrow the plan allocator for the workspace
+  tmp.ctx = ctx;
+  tmp.stream = (cudaStream_t)stream;
+  cudaStream_t st = tmp.stream;
+  spg_status rc = SPG_OK;
+  int32_t* kept = nullptr;
+  int64_t* newptr = nullptr;
+  void* scan_tmp = nullptr;
+  int32_t* tcol = nullptr;
+  double* tval = nullptr;
+  std::vector<int64_t> oldp((size_t)n + 1), newp((size_t)n + 1);
+  do {
+    if ((rc = palloc(&tmp, &kept, n)) != SPG_OK) break;
+    if ((rc = palloc(&tmp, &newptr, (int64_t)n + 1)) != SPG_OK) break;
+    if ((rc = palloc(&tmp, (char**)&scan_tmp, (int64_t)scan_tmp_bytes(n))) != SPG_OK) break;
+    cudaError_t e = launch_count_kept(C->rowptr, C->val, n, kept, st);
+    if (e == cudaSuccess) e = launch_scan_i32_i64(kept, newptr, n, scan_tmp, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(oldp.data(), C->rowptr, sizeof(int64_t) * ((size_t)n + 1),
+                          cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(newp.data(), newptr, sizeof(int64_t) * ((size_t)n + 1),
+                          cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) { rc = cuda_status(e, "drop zeros count"); break; }
+    if (oldp[0] != 0 || oldp[n] != C->nnz) {
+      rc = set_error(SPG_ERR_INVALID_ARG, "row pointers do not match nnz %lld",
+                     (long long)C->nnz);
+      break;
+    }
+    if (newp[n] == C->nnz) break;  // no zero values
+    // row chunks of at most `room` old entries (and at least one row)
+    int64_t room = (int64_t)1 << 25, longest = 0;
+    for (int32_t i = 0; i < n; ++i) longest = std::max(longest, oldp[i + 1] - oldp[i]);
+    room = std::min(std::max(room, longest), C->nnz);
+    if ((rc = palloc(&tmp, &tcol, room)) != SPG_OK) break;
+    if ((rc = palloc(&tmp, &tval, room)) != SPG_OK) break;
+    for (int32_t r0 = 0; r0 < n && rc == SPG_OK;) {
+      int32_t r1 = r0 + 1;
+      while (r1 < n && oldp[r1 + 1] - oldp[r0] <= room) ++r1;
+      e = launch_gather_kept(C->rowptr, C->col, C->val, newptr, r0, r1, tcol, tval, st);
+      const int64_t m = newp[r1] - newp[r0];
+      if (e == cudaSuccess && m > 0)
+        e = cudaMemcpyAsync(C->col + newp[r0], tcol, sizeof(int32_t) * (size_t)m,
+                            cudaMemcpyDeviceToDevice, st);
+      if (e == cudaSuccess && m > 0)
+        e = cudaMemcpyAsync(C->val + newp[r0], tval, sizeof(double) * (size_t)m,
+                            cudaMemcpyDeviceToDevice, st);
+      if (e != cudaSuccess) rc = cuda_status(e, "drop zeros compaction");
+      r0 = r1;
+    }
+    if (rc != SPG_OK) break;
+    e = cudaMemcpyAsync(C->rowptr, newptr, sizeof(int64_t) * ((size_t)n + 1),
+                        cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) { rc = cuda_status(e, "drop zeros row pointers"); break; }
+    C->nnz = newp[n];
+  } while (0);
+  for (void* ptr : tmp.ptrs) cudaFreeAsync(ptr, st);
+  tmp.ptrs.clear();
+  return rc;
+}
+
 spg_status spg_transpose(spg_ctx* ctx, const spg_csr_dev* A, int32_t* t_rowptr, int32_t* t_col,
                          double* t_val, void* stream) {
   begin_call();

@@ -157,6 +157,15 @@ __device__ __forceinline__ int span_bits(int lo, int hi) {
   return span ? 32 - __clz((int)span) : 0;
 }
 
+// Numeric-zero compaction (k_compact.cu): kept (non-zero) entries per row of
+// C, and the kept entries of rows [r0, r1) gathered in order into tcol/tval
+// at newptr[row] − newptr[r0].
+cudaError_t launch_count_kept(const int64_t* rowptr, const double* val, int32_t n, int32_t* kept,
+                              cudaStream_t s);
+cudaError_t launch_gather_kept(const int64_t* rowptr, const int32_t* col, const double* val,
+                               const int64_t* newptr, int32_t r0, int32_t r1, int32_t* tcol,
+                               double* tval, cudaStream_t s);
+
 // Warp-per-row kernels (k_rows_w32.cu) for table bins of up to 2048 slots
 // with 32 lanes per row; returns cudaErrorNotSupported for other bins.
 cudaError_t launch_hash_w32(int log2t, bool numeric, bool gram, const RowArgs& a, int num_sms,

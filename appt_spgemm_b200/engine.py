@@ -313,6 +313,18 @@ class Engine:
                                   tv.data_ptr(), _stream_handle(stream)), "transpose")
         return CsrDevice(A.n, tp, tc[: A.nnz], tv[: A.nnz])
 
+    def drop_zeros(self, C: CsrResult, stream=None) -> CsrResult:
+        """Drop C's exact zero values in place (scipy's eliminate_zeros()
+        pattern); returns C with its nnz and col/val views shortened."""
+        c = SpgCsrOut(C.n, C.nnz, C.rowptr.data_ptr(), C.col.data_ptr() if C.nnz else 0,
+                      C.val.data_ptr() if C.nnz else 0)
+        check(lib().spg_drop_zeros(self._h, ctypes.byref(c), _stream_handle(stream)),
+              "drop zeros")
+        C.nnz = int(c.nnz)
+        C.col = C.col[: C.nnz]
+        C.val = C.val[: C.nnz]
+        return C
+
     def describe(self, A: CsrDevice, stream=None) -> dict:
         d = SpgDescriptors()
         s = A.struct()

@@ -292,6 +292,17 @@ spg_status spg_profile_enable(spg_ctx* ctx, int32_t enable);
 spg_status spg_profile_reset(spg_ctx* ctx);
 spg_status spg_profile_read(spg_ctx* ctx, char* json, size_t capacity);
 
+/* ---- numeric-zero switch ----------------------------------------------------
+ * Drop, in place, the entries of a finished product C whose value is exactly
+ * zero (+0.0 or −0.0), keeping the others in order and updating C->rowptr and
+ * C->nnz: the pattern scipy's eliminate_zeros() leaves.  The products
+ * themselves keep cancelled entries, as the reference and cuSPARSE do
+ * (report/CORRECTNESS_NOTES.md:3-16, :16 names this switch).  Works through
+ * a bounded workspace in row chunks, so any size of C compacts in place; it
+ * synchronizes `stream` once to learn the new size.  On an error C may be
+ * partly compacted. */
+spg_status spg_drop_zeros(spg_ctx* ctx, spg_csr_out* C, void* stream);
+
 /* ---- transpose (CSR → CSR of Aᵀ, counting sort; rows sorted) ------------- */
 /* Replaces k_colcount/k_scatter/build_At (src/spgemm_engine.cuh:37-44,140-146)
  * with a deterministic result.  Caller-owned outputs: rowptr n+1, col/val nnz. */

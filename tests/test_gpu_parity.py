@@ -335,3 +335,50 @@ def test_stencil27_full_size_properties(eng):
     assert G.nnz == P.nnz
     assert torch.equal(G.rowptr, P.rowptr) and torch.equal(G.col, P.col)
     assert torch.equal(G.val.view(torch.int64), P.val.view(torch.int64))
+
+
+def prune(ref):
+    """The oracle's product with exact zeros removed (scipy's eliminate_zeros)."""
+    rp, ci, cx = ref
+    keep = cx != 0.0
+    ck = np.concatenate([[0], np.cumsum(keep)]).astype(np.int64)
+    return ck[rp], ci[keep], cx[keep]
+
+
+def signed_ones(A, seed):
+    """A's pattern with values ±1: products of such matrices cancel often."""
+    rng = np.random.default_rng(seed)
+    return csr.CsrHost(A.n, A.rowptr, A.col, rng.choice([-1.0, 1.0], A.nnz))
+
+
+@pytest.mark.parametrize("task", TASKS)
+def test_drop_zeros_matches_pruned_oracle(eng, task):
+    """The numeric-zero switch leaves exactly the entries scipy keeps, also
+    when the product is compacted through several row chunks."""
+    cases = [signed_ones(csr.stencil27(14, 1), 3), signed_ones(csr.rmat(12, 8, seed=4), 5),
+             csr.CsrHost(2, np.array([0, 2, 4], np.int32), np.array([0, 1, 0, 1], np.int32),
+                         np.array([1.0, 1.0, 1.0, -1.0])),
+             csr.laplace2d(30)]
+    for k, A in enumerate(cases):
+        C = eng.multiply(dev(A), task)
+        before = C.nnz
+        eng.drop_zeros(C)
+        torch.cuda.synchronize()
+        ref = prune(oracle.multiply(A, task))
+        assert_same(C, ref, f"drop_zeros{k}/{task}")
+        assert C.nnz <= before
+        eng.drop_zeros(C)  # idempotent
+        torch.cuda.synchronize()
+        assert_same(C, ref, f"drop_zeros{k}/{task}/again")
+
+
+def test_drop_zeros_multi_chunk(eng):
+    """A product of ±1 values with 42.9M entries: more than one 2^25-entry
+    compaction chunk, about a third of the values exactly zero."""
+    A = signed_ones(csr.stencil27(70, 1), 9)
+    C = eng.multiply(dev(A), "AA")
+    eng.drop_zeros(C)
+    torch.cuda.synchronize()
+    ref = prune(oracle.multiply(A, "AA"))
+    assert C.nnz < len(oracle.multiply(A, "AA")[1])
+    assert_same(C, ref, "drop_zeros/stencil70")
