@@ -54,7 +54,7 @@ class SpgConfig(Structure):
                 ("window_bits", c_int32), ("force_heavy", c_int32), ("sym_load_pct", c_int32),
                 ("num_load_pct", c_int32), ("heavy_split", c_int32),
                 ("pool_release_bytes", c_int64), ("heavy_block_budget", c_int64),
-                ("reserved", c_int64 * 4)]
+                ("grid_sms", c_int64), ("reserved", c_int64 * 3)]
 
 
 class SpgEngResult(Structure):

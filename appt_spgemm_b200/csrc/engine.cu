@@ -34,7 +34,8 @@ struct ProfEntry {
 
 struct spg_ctx {
   int device = 0;
-  int num_sms = 148;
+  int num_sms = 148;               // SMs the launches size grids for (grid_sms or the device's)
+  int device_sms = 148;
   cudaMemPool_t pool = nullptr;
   spg_config cfg{};
   uint32_t* d_status = nullptr;   // device status word (+ scratch, 256 B)
@@ -215,7 +216,13 @@ spg_config merged_config(const spg_config* user) {
       c.lanes_per_row != 16 && c.lanes_per_row != 32)
     c.lanes_per_row = 0;
   if (c.heavy_block_budget <= 0) c.heavy_block_budget = (int64_t)1 << 27;  // 256 MB of counts
+  if (c.grid_sms < 0) c.grid_sms = 0;
+  if (c.grid_sms > (1 << 16)) c.grid_sms = 1 << 16;
   return c;
+}
+
+int grid_sms_of(const spg_config& c, int device_sms) {
+  return c.grid_sms > 0 ? (int)c.grid_sms : device_sms;
 }
 
 constexpr int64_t kHeavySplitDefault = 128;  // mean B-row length
@@ -707,8 +714,9 @@ spg_status spg_create(spg_ctx** out, const spg_config* cfg) {
   spg_status st = SPG_OK;
   do {
     if ((e = cudaSetDevice(dev)) != cudaSuccess) { st = cuda_status(e, "cudaSetDevice"); break; }
-    if ((e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, dev)) !=
+    if ((e = cudaDeviceGetAttribute(&ctx->device_sms, cudaDevAttrMultiProcessorCount, dev)) !=
         cudaSuccess) { st = cuda_status(e, "device attribute"); break; }
+    ctx->num_sms = grid_sms_of(ctx->cfg, ctx->device_sms);
     cudaMemPoolProps props{};
     props.allocType = cudaMemAllocationTypePinned;
     props.location.type = cudaMemLocationTypeDevice;
@@ -960,6 +968,7 @@ spg_status spg_set_config(spg_ctx* ctx, const spg_config* cfg) {
   const int dev = ctx->device;
   ctx->cfg = merged_config(cfg);
   ctx->cfg.device = dev;
+  ctx->num_sms = grid_sms_of(ctx->cfg, ctx->device_sms);
   return SPG_OK;
 }
 

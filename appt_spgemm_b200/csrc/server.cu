@@ -10,9 +10,17 @@
 //    takes the other queued small requests of the same task (up to batch_max)
 //    and runs them as one batched plan (block-diagonal layout), then copies
 //    each request's slice of the result into its own buffers;
-//  - after planning, a request's exact output size plus the plan workspace is
-//    reserved against the budget; the worker waits (condition variable) until
-//    enough is free, and rejects requests that could never fit.
+//  - with two or more workers, worker 0 takes small requests only, so small
+//    requests always have a lane and never queue behind large ones; its stream
+//    has the highest priority and the other workers' launches use one CTA per
+//    work item (no persistent grids), so small requests' CTAs interleave with
+//    a large product's instead of waiting for it to finish;
+//  - after planning, a job's exact output size plus the plan workspace is
+//    reserved against the budget.  A job that can never fit is rejected (a
+//    batch is split into its requests first); a job that does not fit yet is
+//    kept, planned, in the worker's waiting list (at most two) while the
+//    worker takes other work, and runs as soon as releases make room, oldest
+//    first.
 // The reference has no serving layer; this follows the serving contract of
 // the benchmark configuration (Poisson arrivals, p50/p99 latency).
 #include <cuda_runtime.h>
@@ -65,7 +73,7 @@ struct spg_server {
   int device = 0;
   Clock::time_point t0;
   std::mutex mu;
-  std::condition_variable cv_queue, cv_done, cv_budget;
+  std::condition_variable cv_work, cv_done;  // work: queue, budget or stop changed
   std::deque<uint64_t> queue;
   std::unordered_map<uint64_t, std::unique_ptr<Request>> reqs;
   uint64_t next_id = 1;
@@ -86,25 +94,6 @@ void finish(spg_server* s, Request* r, int32_t status, const char* err = nullptr
   r->done_ms = s->now_ms();
 }
 
-// Reserve `need` bytes of the budget, waiting for releases; false when the
-// request can never fit (rejected) or the server stops.
-bool reserve(spg_server* s, std::unique_lock<std::mutex>& lk, int64_t need) {
-  if (need > s->cfg.memory_budget_bytes) return false;
-  s->cv_budget.wait(lk, [&] { return s->stopping || s->reserved + need <= s->cfg.memory_budget_bytes; });
-  if (s->stopping) return false;
-  s->reserved += need;
-  s->peak = std::max(s->peak, s->reserved);
-  return true;
-}
-
-void unreserve(spg_server* s, int64_t bytes) {
-  {
-    std::lock_guard<std::mutex> lk(s->mu);
-    s->reserved -= bytes;
-  }
-  s->cv_budget.notify_all();
-}
-
 spg_status alloc_result(Request* r, int32_t n, int64_t nnz, cudaStream_t st) {
   const size_t nz = (size_t)(nnz > 0 ? nnz : 1);
   cudaError_t e = cudaMallocAsync((void**)&r->rowptr, 8 * ((size_t)n + 1), st);
@@ -122,157 +111,264 @@ void free_result(Request* r, cudaStream_t st) {
   r->val = nullptr;
 }
 
-void run_single(spg_server* s, spg_ctx* ctx, cudaStream_t st, Request* r) {
+// One unit of work: a single request or a merged batch, planned (symbolic
+// done, sizes known) and waiting for its share of the budget.
+struct Job {
+  std::vector<Request*> rs;
   spg_plan* p = nullptr;
-  spg_status rc = spg_plan_create(ctx, r->task, &r->A, st, &p);
-  if (rc != SPG_OK) {
-    std::lock_guard<std::mutex> lk(s->mu);
-    finish(s, r, rc, spg_last_error_string());
-    return;
-  }
   spg_plan_info info{};
-  spg_plan_get_info(p, &info);
-  const int64_t out = output_bytes(r->A.n, info.nnz_c);
-  const int64_t need = out + info.workspace_bytes;
-  {
-    std::unique_lock<std::mutex> lk(s->mu);
-    r->products = info.products;
-    r->nnz_c = info.nnz_c;
-    if (!reserve(s, lk, need)) {
-      if (s->stopping) finish(s, r, SPG_ERR_CUDA, "server stopped before the request ran");
-      else finish(s, r, SPG_ERR_BUDGET, "request exceeds the memory budget");
-      lk.unlock();
-      spg_plan_destroy(p);
-      return;
+  std::vector<int64_t> row_off, nnz_off, out_r;  // merged batches
+  int64_t outs = 0;  // result bytes, reserved until the client releases them
+  int64_t temp = 0;  // workspace (and, for a batch, the concatenated C) for the run
+  int64_t need() const { return outs + temp; }
+};
+
+constexpr size_t kMaxWaiting = 2;  // planned jobs a worker keeps while it takes new work
+
+// Plan `j` (one request or a batch).  Returns false when the job is gone: a
+// single request that failed to plan is finished with the error; a batch
+// that failed to plan is split into single-request jobs appended to `split`.
+bool plan_job(spg_server* s, spg_ctx* ctx, cudaStream_t st, Job& j, std::vector<Job>& split) {
+  if (j.rs.size() == 1) {
+    Request* r = j.rs[0];
+    spg_status rc = spg_plan_create(ctx, r->task, &r->A, st, &j.p);
+    if (rc != SPG_OK) {
+      std::lock_guard<std::mutex> lk(s->mu);
+      finish(s, r, rc, spg_last_error_string());
+      return false;
     }
-    r->reserved = out;
+    spg_plan_get_info(j.p, &j.info);
+    j.outs = output_bytes(r->A.n, j.info.nnz_c);
+    j.temp = j.info.workspace_bytes;
+    std::lock_guard<std::mutex> lk(s->mu);
+    r->products = j.info.products;
+    r->nnz_c = j.info.nnz_c;
+    return true;
   }
-  rc = alloc_result(r, r->A.n, info.nnz_c, st);
-  spg_csr_out C{r->A.n, 0, r->rowptr, r->col, r->val};
-  if (rc == SPG_OK) rc = spg_execute(p, &C, st);
-  if (rc == SPG_OK && cudaStreamSynchronize(st) != cudaSuccess) rc = SPG_ERR_CUDA;
-  const std::string err = rc == SPG_OK ? "" : spg_last_error_string();
-  spg_plan_destroy(p);
-  if (rc != SPG_OK) free_result(r, st);
-  unreserve(s, info.workspace_bytes + (rc == SPG_OK ? 0 : out));
-  std::lock_guard<std::mutex> lk(s->mu);
-  if (rc != SPG_OK) r->reserved = 0;
-  finish(s, r, rc, rc == SPG_OK ? nullptr : err.c_str());
+  std::vector<spg_csr_dev> As;
+  for (Request* r : j.rs) As.push_back(r->A);
+  spg_status rc = spg_plan_create_batched(ctx, j.rs[0]->task, (int32_t)j.rs.size(), As.data(), st,
+                                          &j.p);
+  if (rc != SPG_OK) {  // e.g. one bad instance: plan each alone to isolate it
+    for (Request* r : j.rs) {
+      Job one;
+      one.rs.push_back(r);
+      split.push_back(std::move(one));
+    }
+    return false;
+  }
+  spg_plan_get_info(j.p, &j.info);
+  const size_t b = j.rs.size();
+  j.row_off.resize(b + 1);
+  j.nnz_off.resize(b + 1);
+  j.out_r.resize(b);
+  spg_plan_batch_offsets(j.p, j.row_off.data(), j.nnz_off.data());
+  for (size_t i = 0; i < b; ++i) {
+    j.out_r[i] = output_bytes(j.rs[i]->A.n, j.nnz_off[i + 1] - j.nnz_off[i]);
+    j.outs += j.out_r[i];
+  }
+  j.temp = output_bytes(j.info.n, j.info.nnz_c) + j.info.workspace_bytes;
+  return true;
 }
 
-void run_batch(spg_server* s, spg_ctx* ctx, cudaStream_t st, std::vector<Request*>& rs) {
-  std::vector<spg_csr_dev> As;
-  for (Request* r : rs) As.push_back(r->A);
-  spg_plan* p = nullptr;
-  spg_status rc = spg_plan_create_batched(ctx, rs[0]->task, (int32_t)rs.size(), As.data(), st, &p);
-  if (rc != SPG_OK) {  // e.g. one bad instance: run each alone to isolate it
-    for (Request* r : rs) run_single(s, ctx, st, r);
-    return;
-  }
-  spg_plan_info info{};
-  spg_plan_get_info(p, &info);
-  std::vector<int64_t> row_off(rs.size() + 1), nnz_off(rs.size() + 1);
-  spg_plan_batch_offsets(p, row_off.data(), nnz_off.data());
-  int64_t outs = 0;
-  std::vector<int64_t> out_r(rs.size());
-  for (size_t b = 0; b < rs.size(); ++b) {
-    out_r[b] = output_bytes(rs[b]->A.n, nnz_off[b + 1] - nnz_off[b]);
-    outs += out_r[b];
-  }
-  // the concatenated output and the workspace are temporary
-  const int64_t temp = output_bytes(info.n, info.nnz_c) + info.workspace_bytes;
+// Execute an admitted job (its need is reserved) and finish its requests.
+void run_job(spg_server* s, cudaStream_t st, Job& j) {
+  spg_status rc = SPG_OK;
+  const bool batch = j.rs.size() > 1;
   {
-    std::unique_lock<std::mutex> lk(s->mu);
-    if (!reserve(s, lk, outs + temp)) {
-      lk.unlock();
-      spg_plan_destroy(p);
-      for (Request* r : rs) run_single(s, ctx, st, r);
-      return;
-    }
-    ++s->batches;
-    for (size_t b = 0; b < rs.size(); ++b) {
-      rs[b]->batched = true;
-      rs[b]->reserved = out_r[b];
-      rs[b]->nnz_c = nnz_off[b + 1] - nnz_off[b];
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (batch) ++s->batches;
+    for (size_t b = 0; b < j.rs.size(); ++b) {
+      Request* r = j.rs[b];
+      r->batched = batch;
+      r->reserved = batch ? j.out_r[b] : j.outs;
+      if (batch) r->nnz_c = j.nnz_off[b + 1] - j.nnz_off[b];
     }
   }
-  Request cat;
-  rc = alloc_result(&cat, info.n, info.nnz_c, st);
-  spg_csr_out C{info.n, 0, cat.rowptr, cat.col, cat.val};
-  if (rc == SPG_OK) rc = spg_execute(p, &C, st);
-  for (size_t b = 0; b < rs.size() && rc == SPG_OK; ++b) {
-    Request* r = rs[b];
-    const int64_t nz = nnz_off[b + 1] - nnz_off[b];
-    rc = alloc_result(r, r->A.n, nz, st);
-    if (rc != SPG_OK) break;
-    k_rebase<<<(r->A.n + 256) / 256, 256, 0, st>>>(cat.rowptr, row_off[b], nnz_off[b], r->A.n,
-                                                    r->rowptr);
-    SPG_COUNT_LAUNCH();
-    if (nz > 0) {
-      cudaMemcpyAsync(r->col, cat.col + nnz_off[b], 4 * (size_t)nz, cudaMemcpyDeviceToDevice, st);
-      cudaMemcpyAsync(r->val, cat.val + nnz_off[b], 8 * (size_t)nz, cudaMemcpyDeviceToDevice, st);
+  if (!batch) {
+    Request* r = j.rs[0];
+    rc = alloc_result(r, r->A.n, j.info.nnz_c, st);
+    spg_csr_out C{r->A.n, 0, r->rowptr, r->col, r->val};
+    if (rc == SPG_OK) rc = spg_execute(j.p, &C, st);
+  } else {
+    Request cat;
+    rc = alloc_result(&cat, j.info.n, j.info.nnz_c, st);
+    spg_csr_out C{j.info.n, 0, cat.rowptr, cat.col, cat.val};
+    if (rc == SPG_OK) rc = spg_execute(j.p, &C, st);
+    for (size_t b = 0; b < j.rs.size() && rc == SPG_OK; ++b) {
+      Request* r = j.rs[b];
+      const int64_t nz = j.nnz_off[b + 1] - j.nnz_off[b];
+      rc = alloc_result(r, r->A.n, nz, st);
+      if (rc != SPG_OK) break;
+      k_rebase<<<(r->A.n + 256) / 256, 256, 0, st>>>(cat.rowptr, j.row_off[b], j.nnz_off[b],
+                                                      r->A.n, r->rowptr);
+      SPG_COUNT_LAUNCH();
+      if (nz > 0) {
+        cudaMemcpyAsync(r->col, cat.col + j.nnz_off[b], 4 * (size_t)nz,
+                        cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync(r->val, cat.val + j.nnz_off[b], 8 * (size_t)nz,
+                        cudaMemcpyDeviceToDevice, st);
+      }
     }
+    free_result(&cat, st);
   }
-  free_result(&cat, st);
   if (rc == SPG_OK && cudaStreamSynchronize(st) != cudaSuccess) rc = SPG_ERR_CUDA;
   const std::string err = rc == SPG_OK ? "" : spg_last_error_string();
-  spg_plan_destroy(p);
+  spg_plan_destroy(j.p);
+  j.p = nullptr;
   if (rc != SPG_OK)
-    for (Request* r : rs) free_result(r, st);
-  unreserve(s, temp + (rc == SPG_OK ? 0 : outs));
-  std::lock_guard<std::mutex> lk(s->mu);
-  for (size_t b = 0; b < rs.size(); ++b) {
-    // the product count of an instance: the batch total split by its output share
-    rs[b]->products = info.nnz_c > 0 ? (int64_t)((double)info.products * (double)rs[b]->nnz_c /
-                                                 (double)info.nnz_c) : 0;
-    if (rc != SPG_OK) rs[b]->reserved = 0;
-    finish(s, rs[b], rc, rc == SPG_OK ? nullptr : err.c_str());
+    for (Request* r : j.rs) free_result(r, st);
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->reserved -= j.temp + (rc == SPG_OK ? 0 : j.outs);
+    for (size_t b = 0; b < j.rs.size(); ++b) {
+      Request* r = j.rs[b];
+      if (batch)  // the product count of an instance: the batch total split by output share
+        r->products = j.info.nnz_c > 0 ? (int64_t)((double)j.info.products * (double)r->nnz_c /
+                                                   (double)j.info.nnz_c) : 0;
+      if (rc != SPG_OK) r->reserved = 0;
+      finish(s, r, rc, rc == SPG_OK ? nullptr : err.c_str());
+    }
   }
+  s->cv_work.notify_all();  // budget returned
+  s->cv_done.notify_all();
+}
+
+// Take the oldest queued request this worker may serve (the small-request
+// lane serves only n < batch_rows) and, if it is small, the other queued
+// small requests of the same task, up to batch_max.  Caller holds the lock.
+bool take_requests(spg_server* s, bool small_only, std::vector<Request*>& rs) {
+  auto it = s->queue.begin();
+  for (; it != s->queue.end(); ++it)
+    if (!small_only || s->reqs[*it]->A.n < s->cfg.batch_rows) break;
+  if (it == s->queue.end()) return false;
+  Request* r = s->reqs[*it].get();
+  s->queue.erase(it);
+  rs.push_back(r);
+  if (r->A.n < s->cfg.batch_rows) {
+    for (auto q = s->queue.begin(); q != s->queue.end() && (int)rs.size() < s->cfg.batch_max;) {
+      Request* x = s->reqs[*q].get();
+      if (x->task == r->task && x->A.n < s->cfg.batch_rows) {
+        rs.push_back(x);
+        q = s->queue.erase(q);
+      } else {
+        ++q;
+      }
+    }
+  }
+  const double t = s->now_ms();
+  for (Request* x : rs) x->start_ms = t;
+  return true;
+}
+
+// Admission after planning: reject what can never fit, reserve what fits now,
+// otherwise keep it waiting (with its plan) while the worker takes other work.
+enum class Admit { kRun, kWait, kRejected };
+Admit admit(spg_server* s, Job& j, std::vector<Job>& split) {
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (j.need() > s->cfg.memory_budget_bytes) {
+    if (j.rs.size() > 1) {  // a batch too large for the budget: try its requests one by one
+      for (Request* r : j.rs) {
+        Job one;
+        one.rs.push_back(r);
+        split.push_back(std::move(one));
+      }
+    } else {
+      finish(s, j.rs[0], SPG_ERR_BUDGET, "request exceeds the memory budget");
+    }
+    return Admit::kRejected;
+  }
+  if (s->reserved + j.need() <= s->cfg.memory_budget_bytes) {
+    s->reserved += j.need();
+    s->peak = std::max(s->peak, s->reserved);
+    return Admit::kRun;
+  }
+  return Admit::kWait;
 }
 
 void worker_main(spg_server* s, int index) {
-  (void)index;
   cudaSetDevice(s->device);
+  // with two or more workers, worker 0 serves small requests only, so they
+  // are never queued behind large ones; its stream has the highest priority
+  // and the other workers launch one CTA per work item, so the small
+  // requests' CTAs start as soon as any of the large ones retire
+  const bool small_only = s->cfg.workers >= 2 && index == 0;
+  int least = 0, greatest = 0;
+  cudaDeviceGetStreamPriorityRange(&least, &greatest);
   cudaStream_t st = nullptr;
-  cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, small_only ? greatest : least);
   spg_config cfg{};
   cfg.struct_size = sizeof(spg_config);
   cfg.device = s->device;
   cfg.pool_release_bytes = 64ll << 20;  // give freed memory back: the budget is global
+  if (s->cfg.workers >= 2 && !small_only) cfg.grid_sms = 1 << 16;
   spg_ctx* ctx = nullptr;
   const bool ok = spg_create(&ctx, &cfg) == SPG_OK;
+  std::deque<Job> waiting;  // planned, not admitted yet, oldest first
+  std::vector<Job> todo;    // taken or split off, to be planned
   for (;;) {
-    std::vector<Request*> rs;
-    {
+    Job job;
+    bool run_now = false;
+    if (todo.empty()) {
       std::unique_lock<std::mutex> lk(s->mu);
-      s->cv_queue.wait(lk, [&] { return s->stopping || !s->queue.empty(); });
-      if (s->queue.empty()) break;  // stopping with nothing left
-      Request* r = s->reqs[s->queue.front()].get();
-      s->queue.pop_front();
-      rs.push_back(r);
-      if (r->A.n < s->cfg.batch_rows) {
-        for (auto it = s->queue.begin(); it != s->queue.end() && (int)rs.size() < s->cfg.batch_max;) {
-          Request* q = s->reqs[*it].get();
-          if (q->task == r->task && q->A.n < s->cfg.batch_rows) {
-            rs.push_back(q);
-            it = s->queue.erase(it);
-          } else {
-            ++it;
-          }
+      for (;;) {
+        if (!waiting.empty() &&
+            s->reserved + waiting.front().need() <= s->cfg.memory_budget_bytes) {
+          job = std::move(waiting.front());
+          waiting.pop_front();
+          s->reserved += job.need();
+          s->peak = std::max(s->peak, s->reserved);
+          run_now = true;
+          break;
         }
+        std::vector<Request*> rs;
+        if (waiting.size() < kMaxWaiting && take_requests(s, small_only, rs)) {
+          Job j;
+          j.rs = std::move(rs);
+          todo.push_back(std::move(j));
+          break;
+        }
+        if (s->stopping) break;
+        s->cv_work.wait(lk);
       }
-      const double t = s->now_ms();
-      for (Request* q : rs) q->start_ms = t;
+      if (!run_now && todo.empty()) {  // stopping: what still waits does not run
+        for (Job& j : waiting)
+          for (Request* r : j.rs) finish(s, r, SPG_ERR_CUDA, "server stopped before the request ran");
+        lk.unlock();
+        for (Job& j : waiting) spg_plan_destroy(j.p);
+        waiting.clear();
+        s->cv_done.notify_all();
+        break;
+      }
     }
+    if (run_now) {
+      run_job(s, st, job);
+      continue;
+    }
+    job = std::move(todo.back());
+    todo.pop_back();
     if (!ok) {
       std::lock_guard<std::mutex> lk(s->mu);
-      for (Request* q : rs) finish(s, q, SPG_ERR_CUDA, "worker context could not be created");
-    } else if (rs.size() == 1) {
-      run_single(s, ctx, st, rs[0]);
-    } else {
-      run_batch(s, ctx, st, rs);
+      for (Request* r : job.rs) finish(s, r, SPG_ERR_CUDA, "worker context could not be created");
+      s->cv_done.notify_all();
+      continue;
     }
-    s->cv_done.notify_all();
+    if (!plan_job(s, ctx, st, job, todo)) {
+      s->cv_done.notify_all();
+      continue;
+    }
+    switch (admit(s, job, todo)) {
+      case Admit::kRun:
+        run_job(s, st, job);
+        break;
+      case Admit::kWait:
+        waiting.push_back(std::move(job));
+        break;
+      case Admit::kRejected:
+        spg_plan_destroy(job.p);
+        s->cv_done.notify_all();
+        break;
+    }
   }
   if (ctx) spg_destroy(ctx);
   cudaStreamDestroy(st);
@@ -326,7 +422,7 @@ spg_status spg_server_submit(spg_server* s, spg_task task, const spg_csr_dev* A,
     s->queue.push_back(r->id);
     s->reqs[r->id] = std::move(r);
   }
-  s->cv_queue.notify_one();
+  s->cv_work.notify_all();  // any worker may be the one allowed to take it
   return SPG_OK;
 }
 
@@ -417,7 +513,7 @@ spg_status spg_server_release(spg_server* s, uint64_t id) {
     r->reserved = 0;
     s->reserved -= bytes;
   }
-  s->cv_budget.notify_all();
+  s->cv_work.notify_all();
   return SPG_OK;
 }
 
@@ -466,8 +562,7 @@ spg_status spg_server_destroy(spg_server* s) {
     std::lock_guard<std::mutex> lk(s->mu);
     s->stopping = true;
   }
-  s->cv_queue.notify_all();
-  s->cv_budget.notify_all();
+  s->cv_work.notify_all();
   for (std::thread& t : s->workers) t.join();
   cudaSetDevice(s->device);
   for (auto& kv : s->reqs) free_result(kv.second.get(), nullptr);

@@ -571,14 +571,19 @@ def run_serve(args):
                 st = srv.stats()
             ok = [(k, i) for k, i in done if i["status"] == _capi.SPG_OK]
             lat = sorted(i["done_ms"] - i["submit_ms"] for _, i in ok)
+            small = sorted(i["done_ms"] - i["submit_ms"] for k, i in ok
+                           if pool[int(picks[k])][0].n < 65536)
+
+            def pct(v, q):
+                return round(v[min(len(v) - 1, int(q * len(v)))], 3) if v else None
             work = sum(2.0 * prods[(int(picks[k]), str(tasks[k]))] for k, _ in ok)
             span_s = (max(i["done_ms"] for _, i in ok) - min(i["submit_ms"] for _, i in ok)) / 1e3
             results.append({"rate_per_s": rate, "server": label, "requests": nreq,
                             "completed": len(ok), "rejected": int(st["rejected"]),
                             "failed": int(st["failed"]), "batches": int(st["batches"]),
-                            "p50_ms": round(lat[len(lat) // 2], 3) if lat else None,
-                            "p99_ms": round(lat[min(len(lat) - 1, int(0.99 * len(lat)))], 3)
-                            if lat else None,
+                            "p50_ms": pct(lat, 0.5), "p99_ms": pct(lat, 0.99),
+                            "small_requests": len(small),
+                            "small_p50_ms": pct(small, 0.5), "small_p99_ms": pct(small, 0.99),
                             "sustained_gflops": round(work / span_s / 1e9, 3) if ok else None,
                             "peak_reserved_gb": round(st["peak_reserved_bytes"] / 1e9, 2)})
             print(json.dumps(results[-1]), file=sys.stderr, flush=True)

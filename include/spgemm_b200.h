@@ -109,7 +109,13 @@ typedef struct spg_config {
                                  columns to stay within it, and without them
                                  every heavy row takes the CTA kernel);
                                  0 → 2^27                                       */
-  int64_t reserved[4];
+  int64_t grid_sms;           /* SMs the launches size their persistent grids
+                                 for; 0 → the device's.  A larger value (up to
+                                 2^16) gives one CTA per work item, so CTAs
+                                 retire often and work on a higher-priority
+                                 stream can start in between (the server's
+                                 large-request workers use this)               */
+  int64_t reserved[3];
 } spg_config;
 
 /* Result record of spg_run_ours: the reference's EngResult {ms, nnz, s, as, sq}
