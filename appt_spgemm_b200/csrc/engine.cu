@@ -394,10 +394,10 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
     ProfScope ps(ctx, "plan/bin_sym", st);
     TRY_CUDA(launch_bin_rows(bsym, hist, counts, rows_sym, st), "symbolic binning");
   }
-  // column blocks of the heavy rows: 1024 columns, so that a block never
-  // holds more distinct columns than a window (cap >= 1024 at the default
-  // load) and windows are packed from the counts alone; wider when that many
-  // counts would exceed kHeavyBlockBudget (chosen after the readback below)
+  // column blocks of the heavy rows: 1024 columns (windows are packed from
+  // the counts; a block above the window cap, 675 columns at the default
+  // load, is cut into fixed 512-column windows); wider when that many counts
+  // would exceed heavy_block_budget (chosen after the readback below)
   p->blk_log2 = 10;
   int32_t* nblk;
   void* btmp;

@@ -223,7 +223,7 @@ cudaError_t launch_heavy_blocks(const BinSource& bsym, int blk_log2, int32_t* nb
 // Windowed numeric phase of heavy rows (k_heavy_w32.cu): a warp per row walks
 // the row's column blocks in windows of at most `cap` distinct columns.
 cudaError_t launch_heavy_w32(bool gram, const HeavyArgs& a, int num_sms, cudaStream_t s);
-constexpr int kHeavyTableLog2 = 11;  // its shared table: 2048 slots per warp
+constexpr int kHeavyTableLog2 = 10;  // its shared table: 1024 slots per warp
 
 // ---- transpose and segment sort (k_transpose.cu) ----------------------------
 
