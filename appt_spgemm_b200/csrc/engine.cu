@@ -144,6 +144,8 @@ struct spg_plan {
   uint16_t* blk_cnt = nullptr;
   int blk_log2 = 12;
   int4* hcur = nullptr;
+  int window_bits = 1 << 20;  // heavy-path shape (heavy_shape)
+  int heavy_threads = 1024;
 };
 
 struct spg_graph {
@@ -202,11 +204,12 @@ spg_config merged_config(const spg_config* user) {
   }
   c.struct_size = sizeof(spg_config);
   if (c.max_smem_slots <= 0) c.max_smem_slots = 8192;
-  if (c.heavy_threads <= 0) c.heavy_threads = 1024;
+  // 0 = chosen per plan from n (heavy_shape)
+  if (c.heavy_threads < 0) c.heavy_threads = 0;
   if (c.heavy_threads > 1024) c.heavy_threads = 1024;
   c.heavy_threads = (c.heavy_threads + 31) / 32 * 32;
   // windows are whole 4-word groups and fit the shared bitmap (≤ 2^20 bits)
-  if (c.window_bits <= 0) c.window_bits = 1 << 20;
+  if (c.window_bits < 0) c.window_bits = 0;
   if (c.window_bits > (1 << 20)) c.window_bits = 1 << 20;
   c.window_bits = (c.window_bits + 1023) / 1024 * 1024;
   auto clamp_pct = [](int32_t v, int32_t dflt) { return v <= 0 ? dflt : (v < 20 ? 20 : (v > 90 ? 90 : v)); };
@@ -219,6 +222,21 @@ spg_config merged_config(const spg_config* user) {
   if (c.grid_sms < 0) c.grid_sms = 0;
   if (c.grid_sms > (1 << 16)) c.grid_sms = 1 << 16;
   return c;
+}
+
+// Heavy-path shape of a plan: the bitmap window covers the whole column range
+// when it can (next power of two >= n, at most 2^20), and windows of up to
+// 2^19 columns run 512-thread CTAs, two per SM, so one CTA's barrier waits
+// overlap the other's work (R-MAT 2^18: heavy numeric 80.6 -> 70.4 ms); a
+// 2^20 window keeps one 1024-thread CTA per SM.  Explicit config values win.
+void heavy_shape(const spg_config& c, int32_t n, int* window_bits, int* threads) {
+  int wb = c.window_bits;
+  if (wb <= 0) {
+    wb = 1024;
+    while (wb < n && wb < (1 << 20)) wb <<= 1;
+  }
+  *window_bits = wb;
+  *threads = c.heavy_threads > 0 ? c.heavy_threads : (wb <= (1 << 19) ? 512 : 1024);
 }
 
 int grid_sms_of(const spg_config& c, int device_sms) {
@@ -399,6 +417,7 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
   // load, is cut into fixed 512-column windows); wider when that many counts
   // would exceed heavy_block_budget (chosen after the readback below)
   p->blk_log2 = 10;
+  heavy_shape(ctx->cfg, n, &p->window_bits, &p->heavy_threads);
   int32_t* nblk;
   void* btmp;
   TRY(palloc(p, &nblk, n));
@@ -425,7 +444,7 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
   const int64_t heavy_sym = sym_count[kHeavyBin];
   const int64_t budget = ctx->cfg.heavy_block_budget;
   while (total_blocks > budget && p->blk_log2 < 20 &&
-         ctx->cfg.window_bits % (2 << p->blk_log2) == 0) {
+         p->window_bits % (2 << p->blk_log2) == 0) {
     ++p->blk_log2;
     total_blocks = (hp[2 * kNumBins] >> (p->blk_log2 - 10)) + heavy_sym;
   }
@@ -469,12 +488,12 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
     h.r.nrows = (int32_t)sym_count[kHeavyBin];
     h.lo = p->lo;
     h.hi = p->hi;
-    h.window_bits = ctx->cfg.window_bits;
+    h.window_bits = p->window_bits;
     h.blk_off = p->blk_off;
     h.blk_cnt = p->blk_cnt;
     h.blk_log2 = p->blk_log2;
     ProfScope ps(ctx, "sym/heavy", st);
-    TRY_CUDA(launch_heavy(false, gram, h, ctx->cfg.heavy_threads, ctx->num_sms, st),
+    TRY_CUDA(launch_heavy(false, gram, h, p->heavy_threads, ctx->num_sms, st),
              "symbolic heavy");
   }
 
@@ -626,7 +645,7 @@ spg_status execute_impl(spg_plan* p, spg_csr_out* C, cudaStream_t st) {
       h.r.nrows = (int32_t)p->num_count[kHeavyBin];
       h.lo = p->lo;
       h.hi = p->hi;
-      h.window_bits = ctx->cfg.window_bits;
+      h.window_bits = p->window_bits;
       h.blk_off = p->blk_off;
       h.blk_cnt = p->blk_cnt;
       h.blk_log2 = p->blk_log2;
@@ -645,7 +664,7 @@ spg_status execute_impl(spg_plan* p, spg_csr_out* C, cudaStream_t st) {
       cudaError_t e = cudaSuccess;
       if (windows) e = launch_heavy_w32(gram, h, ctx->num_sms, st);
       if (e == cudaSuccess)
-        e = launch_heavy(true, gram, h, ctx->cfg.heavy_threads, ctx->num_sms, st);
+        e = launch_heavy(true, gram, h, p->heavy_threads, ctx->num_sms, st);
       if (e != cudaSuccess) { result = cuda_status(e, "numeric heavy"); break; }
     }
     if (gram && p->nnz_low > 0) {

@@ -88,10 +88,13 @@ typedef struct spg_config {
                                  0 → chosen from the mean row length of B        */
   int32_t max_smem_slots;     /* largest shared-memory numeric table (slots);
                                  rows beyond go to the heavy path; 0 → 8192      */
-  int32_t heavy_threads;      /* threads per CTA on the heavy path; 0 → 1024     */
+  int32_t heavy_threads;      /* threads per CTA on the heavy path; 0 → 512 when
+                                 the window is ≤ 2^19 columns (two CTAs per SM),
+                                 else 1024                                       */
   int32_t window_bits;        /* column-window width of the dense heavy path
                                  (bits of the shared bitmap, multiple of 1024,
-                                 at most 2^20); 0 → 2^20                         */
+                                 at most 2^20); 0 → the next power of two ≥ n,
+                                 at most 2^20                                    */
   int32_t force_heavy;        /* 1 → send every non-empty row to the heavy path
                                  (debug oracle of the binning, as the reference
                                  did by forcing its global path)                 */
