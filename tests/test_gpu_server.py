@@ -77,3 +77,37 @@ def test_server_budget_rejects_and_holds_back():
         srv.release(r1)
         assert srv.wait(r2, 60000)["status"] == _capi.SPG_OK
         assert srv.stats()["peak_reserved_bytes"] <= int(out_big * 1.6)
+
+
+def test_small_requests_pass_a_large_one_waiting_for_budget():
+    """A large request that does not fit the budget yet waits, planned, while
+    the workers (and the small-request lane) keep serving small requests; it
+    runs once the client releases the result that holds the budget."""
+    from appt_spgemm_b200.engine import Server
+    big = csr.rmat(15, 16, seed=11)               # n = 32768 >= batch_rows below: a large request
+    out_big = 8 * (big.n + 1) + 12 * len(oracle.multiply(big, "AA")[1])
+    smalls = [csr.laplace2d(20 + i) for i in range(12)]
+    with Server(workers=3, memory_budget_bytes=int(out_big * 1.5), batch_rows=4096,
+                batch_max=4) as srv:
+        d = dev(big)
+        r1 = srv.submit(d, "AA")
+        assert srv.wait(r1, 60000)["status"] == _capi.SPG_OK
+        r2 = srv.submit(d, "AA")                 # cannot fit until r1 is released
+        ids = [srv.submit(dev(A), "AA") for A in smalls]
+        for A, rid in zip(smalls, ids):
+            info = srv.wait(rid, 60000)
+            assert info["status"] == _capi.SPG_OK
+            g = srv.result(rid).to_host()
+            o = oracle.multiply(A, "AA")
+            for x, z in zip(g, o):
+                assert np.array_equal(x.view(np.uint8), np.ascontiguousarray(z).view(np.uint8))
+            srv.release(rid)
+        assert srv.poll(r2)["status"] == _capi.SPG_ERR_NOT_READY
+        srv.release(r1)
+        assert srv.wait(r2, 60000)["status"] == _capi.SPG_OK
+        g = srv.result(r2).to_host()
+        o = oracle.multiply(big, "AA")
+        for x, z in zip(g, o):
+            assert np.array_equal(x.view(np.uint8), np.ascontiguousarray(z).view(np.uint8))
+        srv.release(r2)
+        assert srv.stats()["rejected"] == 0
