@@ -405,9 +405,16 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
   TRY(palloc(p, &rows_sym, n));
   const int force = ctx->cfg.force_heavy ? 1 : 0;
   const int num_lg = table_log2_cap(ctx->cfg.max_smem_slots);
+  // short-B-row rows beyond the warp kernel's largest table go heavy too
+  // (windowed warp kernel), with the same mean-length rule as the heavy split
+  const int64_t split = ctx->cfg.heavy_split > 0 ? (int64_t)ctx->cfg.heavy_split
+                                                 : kHeavySplitDefault;
+  const int short_lg = std::min(num_lg, 11);
   BinSource bsym{0, n, p->f, p->lo, p->hi, nullptr, nullptr, kMaxTableLog2, force,
                  ctx->cfg.sym_load_pct,
-                 numeric_heavy_min(num_lg, ctx->cfg.num_load_pct)};
+                 numeric_heavy_min(num_lg, ctx->cfg.num_load_pct),
+                 p->A.rowptr, split, short_lg,
+                 numeric_heavy_min(short_lg, ctx->cfg.num_load_pct)};
   {
     ProfScope ps(ctx, "plan/bin_sym", st);
     TRY_CUDA(launch_bin_rows(bsym, hist, counts, rows_sym, st), "symbolic binning");
@@ -515,7 +522,7 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
   // numeric binning by exact counts, stats; host sync #3 (nnz(C))
   TRY(palloc(p, &p->rows_num, n));
   BinSource bnum{1, n, p->f, p->lo, p->hi, p->rownnz, gram ? p->rowlow : nullptr, num_lg, force,
-                 ctx->cfg.num_load_pct};
+                 ctx->cfg.num_load_pct, 0, p->A.rowptr, split, short_lg, 0};
   {
     ProfScope ps(ctx, "plan/bin_num", st);
     TRY_CUDA(launch_bin_rows(bnum, hist, counts + 2 * kNumBins, p->rows_num, st),

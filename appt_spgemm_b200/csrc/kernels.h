@@ -43,6 +43,15 @@ struct BinSource {
   // every row the numeric binning sends to the heavy path has block counts
   // from the heavy symbolic kernel (0: no such rule)
   int64_t heavy_min;
+  // rows fed by short B rows (products < short_split × nnz(A row); 0: no such
+  // rule) go heavy already above 2^short_max_log2 slots (numeric) or from
+  // min(products, span) >= short_min (symbolic): the windowed warp kernel
+  // serves them better than the CTA-per-row tables, whose per-k barrier idles
+  // most of the CTA on short B rows
+  const int32_t* arowptr;
+  int64_t short_split;
+  int short_max_log2;
+  int64_t short_min;
 };
 
 __host__ __device__ __forceinline__ int ceil_log2_64(int64_t x) {
@@ -73,6 +82,10 @@ __host__ __device__ __forceinline__ int row_bin(const BinSource& s, int i) {
   int lg = ceil_log2_64(want);
   if (lg < kMinTableLog2) lg = kMinTableLog2;
   if (lg > s.max_log2) return kHeavyBin;
+  if (s.short_split > 0 &&
+      s.f[i] < s.short_split * ((int64_t)s.arowptr[i + 1] - s.arowptr[i]) &&
+      (s.mode == 0 ? size >= s.short_min : lg > s.short_max_log2))
+    return kHeavyBin;
   return lg - kMinTableLog2 + 1;
 }
 
