@@ -84,8 +84,14 @@ __device__ __forceinline__ void insert_acc(int* keys, double* vals, int j, doubl
     old = atomicCAS(keys + h, kEmptyKey, j);
   }
   if (NUMERIC) {
+#ifdef SPG_PRED_LOAD
+    double cur = 0.0;
+    if (old != kEmptyKey) cur = vals[h];
+    vals[h] = __dadd_rn(cur, v);
+#else
     const double cur = vals[h];
     vals[h] = __dadd_rn(old == kEmptyKey ? 0.0 : cur, v);
+#endif
   }
 }
 
