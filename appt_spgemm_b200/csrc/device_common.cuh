@@ -66,8 +66,8 @@ __device__ __forceinline__ int hash_insert(int* keys, int j, uint32_t* status) {
 // loop exits on an empty slot (claimed) or on the key itself (reading the slot
 // first and claiming only empty ones measured slower: 3.32 vs 2.88 ms for the
 // numeric phase of the 96³ stencil).  In the numeric phase the value is then
-// 0.0 + v for a freshly claimed slot and slot + v otherwise — a select, not a
-// branch — so no value array is cleared between rows.
+// 0.0 + v for a freshly claimed slot and slot + v otherwise, so no value array
+// is cleared between rows.
 template <int LOG2T, bool NUMERIC>
 __device__ __forceinline__ void insert_acc(int* keys, double* vals, int j, double v,
                                            uint32_t* status) {
@@ -84,14 +84,10 @@ __device__ __forceinline__ void insert_acc(int* keys, double* vals, int j, doubl
     old = atomicCAS(keys + h, kEmptyKey, j);
   }
   if (NUMERIC) {
-#ifdef SPG_PRED_LOAD
+    // a freshly claimed slot starts from 0.0 without reading the stale value
     double cur = 0.0;
     if (old != kEmptyKey) cur = vals[h];
     vals[h] = __dadd_rn(cur, v);
-#else
-    const double cur = vals[h];
-    vals[h] = __dadd_rn(old == kEmptyKey ? 0.0 : cur, v);
-#endif
   }
 }
 
