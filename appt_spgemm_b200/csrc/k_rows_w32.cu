@@ -14,7 +14,7 @@
 //  - packs each occupied slot as ((col − lo) << log2T) | slot, sorts the
 //    packed words with a register bitonic network (E words per lane), and
 //    writes columns and the gathered values to the row's CSR slots; rows of
-//    more than 256 entries (tables of 512 slots and up) sort the packed words
+//    more than 128 entries in tables of 512 slots and up sort the packed words
 //    with a stable LSD radix sort over the column bits instead, O(m) per
 //    digit rather than the bitonic network's O(m log² m), in the table's own
 //    free space.
@@ -29,6 +29,10 @@ namespace spg {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
+// Rows of more entries than this sort with the radix sort rather than the
+// register bitonic network (whose 8-per-lane form costs about 1,000 warp
+// instructions a row against about 600 for two or three digit passes).
+constexpr int kRadixMin = 128;
 
 // Shared memory of one warp's row: the table's values (numeric) and keys.
 template <int LOG2T, bool NUMERIC>
@@ -132,8 +136,9 @@ __global__ void __launch_bounds__(256, 5) k_hash_w32(RowArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   constexpr int T = 1 << LOG2T;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  // rows of more than 256 entries (tables of 512 slots and up) take the radix
-  // sort, with DBITS-bit digits whose counters fit the table's free tail
+  // rows of more than kRadixMin entries in tables of 512 slots and up take the
+  // radix sort, with DBITS-bit digits whose counters fit the table's free tail
+  // (in the 256-slot kernel, the stencil's, the radix code alone cost 3.7%)
   constexpr bool RADIX = NUMERIC && LOG2T >= 9;
   constexpr int DBITS = LOG2T == 9 ? 7 : 8;
   unsigned char* base_p = smem + (size_t)w * w32_warp_bytes<LOG2T, NUMERIC>();
@@ -263,7 +268,7 @@ __global__ void __launch_bounds__(256, 5) k_hash_w32(RowArgs a) {
     // vals; the sort's second buffer (m words) then lives in vals[m..T) and
     // its 2^DBITS counters in keys[m..T), which needs 3m <= 2T and
     // m + 2^DBITS <= T (true up to a 66% table load).
-    const bool radix = RADIX && packs && expect > 256 && 3 * expect <= 2 * T &&
+    const bool radix = RADIX && packs && expect > kRadixMin && 3 * expect <= 2 * T &&
                        expect + (1 << DBITS) <= T;
     if (!packs || (expect > 256 && !radix)) {
       pair_sort_write<LOG2T, GRAM>(a, row, keys, vals, base, expect);
