@@ -24,53 +24,73 @@ constexpr size_t kHeavyScratch = 256;
 
 size_t heavy_smem_bytes(bool numeric, int threads, int window_bits) {
   const size_t words = (size_t)window_bits / 32;
-  size_t b = words * 4 + (size_t)threads * 8 + kHeavyScratch;
+  size_t b = words * 4 + (size_t)threads * 12 + kHeavyScratch;  // + staging of B rows
   if (numeric) b += words + (size_t)threads * 8;  // 4-word group prefixes, staged a_ik
   return b;
 }
 
+// B rows at least this long are marked by the whole CTA, shorter ones by one
+// warp each.
+constexpr int kLongBRow = 256;
+
 // Mark the columns of row `row` that fall in [w0, w0 + 32·nwords) (and, for
-// the Gram upper part, are >= row) in the shared bitmap.  Products are
-// enumerated flat over chunks of blockDim entries of A's row.
+// the Gram upper part, are >= row) in the shared bitmap.  Marking is an OR, so
+// the B rows need no order: per chunk of blockDim entries of A's row, the
+// long B rows (listed in st_long) are swept by the whole CTA one after another
+// and the short ones are dealt out to the warps, a B row per warp — no search
+// for the B row of a product.
 __device__ __forceinline__ void mark_window(const RowArgs& a, int row, long long w0, int nwords,
-                                            uint32_t* bm, int* st_bs, int* st_ex, void* scratch) {
+                                            uint32_t* bm, int* st_bs, int* st_len, int* st_long,
+                                            void* scratch) {
   const int32_t ps = a.A.rowptr[row], pe = a.A.rowptr[row + 1];
   const long long wbits = (long long)nwords * 32;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nwarps = blockDim.x >> 5;
+  int* nlong_p = (int*)scratch;
   for (int32_t pb = ps; pb < pe; pb += blockDim.x) {
     const int cnt = min((int)blockDim.x, pe - pb);
     int bs = 0, len = 0;
-    if ((int)threadIdx.x < cnt) {
-      const int32_t k = a.A.col[pb + threadIdx.x];
+    if (tid < cnt) {
+      const int32_t k = a.A.col[pb + tid];
       bs = a.B.rowptr[k];
       len = a.B.rowptr[k + 1] - bs;
     }
-    int tot;
-    const int ex = block_exclusive_scan(len, (int*)scratch, &tot);
-    st_bs[threadIdx.x] = bs;
-    st_ex[threadIdx.x] = ex;
+    st_bs[tid] = bs;
+    st_len[tid] = len;
+    if (tid == 0) *nlong_p = 0;
     __syncthreads();
-    for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
-      int l = 0, h = cnt - 1;  // largest t with st_ex[t] <= idx
-      while (l < h) {
-        const int mid = (l + h + 1) >> 1;
-        if (st_ex[mid] <= idx) l = mid; else h = mid - 1;
+    if (len >= kLongBRow) st_long[atomicAdd(nlong_p, 1)] = tid;
+    __syncthreads();
+    const int nlong = *nlong_p;
+    for (int i = 0; i < nlong; ++i) {
+      const int t = st_long[i];
+      const int32_t b = st_bs[t], l = st_len[t];
+      for (int q = tid; q < l; q += blockDim.x) {
+        const long long d = (long long)a.B.col[b + q] - w0;
+        if (d >= 0 && d < wbits) atomicOr(&bm[d >> 5], 1u << (d & 31));
       }
-      const long long d = (long long)a.B.col[st_bs[l] + idx - st_ex[l]] - w0;
-      if (d >= 0 && d < wbits) atomicOr(&bm[d >> 5], 1u << (d & 31));
     }
-    __syncthreads();
+    for (int t = wid; t < cnt; t += nwarps) {
+      const int32_t b = st_bs[t], l = st_len[t];
+      if (l >= kLongBRow) continue;
+      for (int q = lane; q < l; q += 32) {
+        const long long d = (long long)a.B.col[b + q] - w0;
+        if (d >= 0 && d < wbits) atomicOr(&bm[d >> 5], 1u << (d & 31));
+      }
+    }
+    __syncthreads();  // staging and the long-row count are reused by the next chunk
   }
 }
 
 template <bool GRAM>
-__global__ void __launch_bounds__(1024) k_heavy_sym(HeavyArgs h) {
+__global__ void __launch_bounds__(1024, 1) k_heavy_sym(HeavyArgs h) {
   extern __shared__ __align__(16) unsigned char smem[];
   const RowArgs& a = h.r;
   const int nw_max = h.window_bits / 32;
   uint32_t* bm = (uint32_t*)smem;
   int* st_bs = (int*)(bm + nw_max);
   int* st_ex = st_bs + blockDim.x;
-  void* scratch = (void*)(st_ex + blockDim.x);
+  int* st_long = st_ex + blockDim.x;
+  void* scratch = (void*)(st_long + blockDim.x);
   for (int r = blockIdx.x; r < a.nrows; r += gridDim.x) {
     const int row = a.rows[r];
     const int lo = h.lo[row], hi = h.hi[row];
@@ -79,7 +99,7 @@ __global__ void __launch_bounds__(1024) k_heavy_sym(HeavyArgs h) {
       const int nwords = (int)min((long long)nw_max, (hi - w0) / 32 + 1);
       for (int i = threadIdx.x; i < nwords; i += blockDim.x) bm[i] = 0u;
       __syncthreads();
-      mark_window(a, row, w0, nwords, bm, st_bs, st_ex, scratch);
+      mark_window(a, row, w0, nwords, bm, st_bs, st_ex, st_long, scratch);
       // a warp per column block of the window (32 or more words): the bit
       // counts are the row totals and, when asked for, the block counts
       int lc = 0, lcl = 0;
@@ -124,7 +144,7 @@ __device__ __forceinline__ int window_rank(const uint32_t* bm, const int* pre4, 
 }
 
 template <bool GRAM>
-__global__ void __launch_bounds__(1024) k_heavy_num(HeavyArgs h) {
+__global__ void __launch_bounds__(1024, 1) k_heavy_num(HeavyArgs h) {
   extern __shared__ __align__(16) unsigned char smem[];
   const RowArgs& a = h.r;
   const int nw_max = h.window_bits / 32;
@@ -134,7 +154,8 @@ __global__ void __launch_bounds__(1024) k_heavy_num(HeavyArgs h) {
   double* st_a = (double*)(pre4 + nw_max / 4);
   int* st_bs = (int*)(st_a + HT);
   int* st_ex = st_bs + HT;
-  void* scratch = (void*)(st_ex + HT);
+  int* st_long = st_ex + HT;
+  void* scratch = (void*)(st_long + HT);
   const int tid = threadIdx.x;
   for (int r = blockIdx.x; r < a.nrows; r += gridDim.x) {
     const int row = a.rows[r];
@@ -151,7 +172,7 @@ __global__ void __launch_bounds__(1024) k_heavy_num(HeavyArgs h) {
       const int ngroups = (nwords + 3) >> 2;
       for (int i = tid; i < ngroups * 4; i += HT) bm[i] = 0u;
       __syncthreads();
-      mark_window(a, row, w0, nwords, bm, st_bs, st_ex, scratch);
+      mark_window(a, row, w0, nwords, bm, st_bs, st_ex, st_long, scratch);
       // exclusive prefix of the bit counts per group of 4 words
       const int per = (ngroups + HT - 1) / HT;
       const int gb = min(ngroups, tid * per), ge = min(ngroups, gb + per);
