@@ -240,13 +240,30 @@ __global__ void __launch_bounds__(1024, 1) k_heavy_num(HeavyArgs h) {
                 a.cval[base + pos] = __dadd_rn(a.cval[base + pos], __dmul_rn(av, bv));
             }
           }
-          for (int q = tid + HT; q < len; q += HT) {
-            const long long d = (long long)a.B.col[bs + q] - w0;
-            if (d >= 0 && d < wbits) {
-              const long long pos = written + window_rank(bm, pre4, d);
-              if (pos < expect)
-                a.cval[base + pos] = __dadd_rn(a.cval[base + pos], __dmul_rn(av, a.B.val[bs + q]));
+          // the rest of a long B row, four entries per thread at a time: their
+          // loads, then their read-modify-writes of C, are issued together
+          // (the entries of one B row are distinct columns)
+          for (int q0 = tid + HT; q0 < len; q0 += 4 * HT) {
+            long long pos[4];
+            double bv4[4], cur[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              const int q = q0 + u * HT;
+              pos[u] = -1;
+              bv4[u] = 0.0;
+              if (q < len) {
+                const long long d = (long long)a.B.col[bs + q] - w0;
+                bv4[u] = a.B.val[bs + q];
+                if (d >= 0 && d < wbits) pos[u] = written + window_rank(bm, pre4, d);
+              }
             }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+              cur[u] = (pos[u] >= 0 && pos[u] < expect) ? a.cval[base + pos[u]] : 0.0;
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+              if (pos[u] >= 0 && pos[u] < expect)
+                a.cval[base + pos[u]] = __dadd_rn(cur[u], __dmul_rn(av, bv4[u]));
           }
           __syncthreads();
         }
