@@ -125,6 +125,17 @@ struct Job {
 
 constexpr size_t kMaxWaiting = 2;  // planned jobs a worker keeps while it takes new work
 
+// Queue the requests of batch `j` as single-request jobs.  The worker takes
+// jobs from the back of `split`, so they go in newest first and run in
+// submission order.
+void split_into_requests(const Job& j, std::vector<Job>& split) {
+  for (auto it = j.rs.rbegin(); it != j.rs.rend(); ++it) {
+    Job one;
+    one.rs.push_back(*it);
+    split.push_back(std::move(one));
+  }
+}
+
 // Plan `j` (one request or a batch).  Returns false when the job is gone: a
 // single request that failed to plan is finished with the error; a batch
 // that failed to plan is split into single-request jobs appended to `split`.
@@ -150,11 +161,7 @@ bool plan_job(spg_server* s, spg_ctx* ctx, cudaStream_t st, Job& j, std::vector<
   spg_status rc = spg_plan_create_batched(ctx, j.rs[0]->task, (int32_t)j.rs.size(), As.data(), st,
                                           &j.p);
   if (rc != SPG_OK) {  // e.g. one bad instance: plan each alone to isolate it
-    for (Request* r : j.rs) {
-      Job one;
-      one.rs.push_back(r);
-      split.push_back(std::move(one));
-    }
+    split_into_requests(j, split);
     return false;
   }
   spg_plan_get_info(j.p, &j.info);
@@ -268,11 +275,7 @@ Admit admit(spg_server* s, Job& j, std::vector<Job>& split) {
   std::lock_guard<std::mutex> lk(s->mu);
   if (j.need() > s->cfg.memory_budget_bytes) {
     if (j.rs.size() > 1) {  // a batch too large for the budget: try its requests one by one
-      for (Request* r : j.rs) {
-        Job one;
-        one.rs.push_back(r);
-        split.push_back(std::move(one));
-      }
+      split_into_requests(j, split);
     } else {
       finish(s, j.rs[0], SPG_ERR_BUDGET, "request exceeds the memory budget");
     }

@@ -111,3 +111,42 @@ def test_small_requests_pass_a_large_one_waiting_for_budget():
             assert np.array_equal(x.view(np.uint8), np.ascontiguousarray(z).view(np.uint8))
         srv.release(r2)
         assert srv.stats()["rejected"] == 0
+
+
+def test_batch_over_budget_is_split_into_requests():
+    """Small requests merged into a batch whose outputs together exceed the
+    budget are split and run one by one, each within the budget."""
+    from appt_spgemm_b200.engine import Server
+    mats = [csr.stencil27(30, 20 + i) for i in range(4)]
+    out = 8 * (mats[0].n + 1) + 12 * len(oracle.multiply(mats[0], "AA")[1])
+    ds = [dev(A) for A in mats]
+    with Server(workers=1, memory_budget_bytes=int(out * 2.5), batch_rows=1 << 20,
+                batch_max=8) as srv:
+        ids = [srv.submit(d, "AA") for d in ds]
+        for A, rid in zip(mats, ids):
+            info = srv.wait(rid, 60000)
+            assert info["status"] == _capi.SPG_OK
+            assert not info["batched"]
+            g = srv.result(rid).to_host()
+            o = oracle.multiply(A, "AA")
+            for x, z in zip(g, o):
+                assert np.array_equal(x.view(np.uint8), np.ascontiguousarray(z).view(np.uint8))
+            srv.release(rid)
+        assert srv.stats()["rejected"] == 0
+
+
+@pytest.mark.timeout(120, method="thread")
+def test_close_with_a_request_waiting_for_budget():
+    """Closing the server while a planned request still waits for budget
+    ends that request with an error status instead of hanging."""
+    from appt_spgemm_b200.engine import Server
+    big = csr.stencil27(40, 8)
+    out_big = 8 * (big.n + 1) + 12 * len(oracle.multiply(big, "AA")[1])
+    srv = Server(workers=2, memory_budget_bytes=int(out_big * 1.6), batch_rows=1)
+    d = dev(big)
+    r1 = srv.submit(d, "AA")
+    assert srv.wait(r1, 60000)["status"] == _capi.SPG_OK
+    r2 = srv.submit(d, "AA")
+    with pytest.raises(_capi.SpgemmError):
+        srv.wait(r2, timeout_ms=1000)
+    srv.close()
