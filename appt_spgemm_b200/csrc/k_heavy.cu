@@ -146,8 +146,16 @@ __device__ __forceinline__ int window_rank(const uint32_t* bm, const int* pre4, 
   return r + __popc(bm[i] & ((1u << b) - 1u));
 }
 
-template <bool GRAM>
-__global__ void __launch_bounds__(1024, 1) k_heavy_num(HeavyArgs h) {
+// Launched with up to 512 threads the kernel is built for three CTAs per SM
+// (40 registers, no spills), so windows of up to 2^18 columns (about 51 KB of
+// shared memory) are not held to two CTAs per SM by registers.  R-MAT 2^17,
+// A·A / A·Aᵀ: 27.1 / 29.1 -> 24.0 / 24.3 ms; 2^18: 64.9 / 65.7 -> 60.6 / 63.0
+// ms.  Four CTAs per SM (32 registers, small spills) were slower: 29.1 and
+// 90.4 ms for A·A.
+constexpr int kNumMinBlocks512 = 3;
+
+template <bool GRAM, int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB) k_heavy_num(HeavyArgs h) {
   extern __shared__ __align__(16) unsigned char smem[];
   const RowArgs& a = h.r;
   const int nw_max = h.window_bits / 32;
@@ -337,9 +345,12 @@ cudaError_t launch_heavy(bool numeric, bool gram, const HeavyArgs& h, int thread
                          cudaStream_t s) {
   if (h.r.nrows <= 0) return cudaSuccess;
   const size_t smem = heavy_smem_bytes(numeric, threads, h.window_bits);
+  if (numeric && threads <= 512)
+    return gram ? launch_h(k_heavy_num<true, 512, kNumMinBlocks512>, threads, smem, h, num_sms, s)
+                : launch_h(k_heavy_num<false, 512, kNumMinBlocks512>, threads, smem, h, num_sms, s);
   if (numeric)
-    return gram ? launch_h(k_heavy_num<true>, threads, smem, h, num_sms, s)
-                : launch_h(k_heavy_num<false>, threads, smem, h, num_sms, s);
+    return gram ? launch_h(k_heavy_num<true, 1024, 1>, threads, smem, h, num_sms, s)
+                : launch_h(k_heavy_num<false, 1024, 1>, threads, smem, h, num_sms, s);
   return gram ? launch_h(k_heavy_sym<true>, threads, smem, h, num_sms, s)
               : launch_h(k_heavy_sym<false>, threads, smem, h, num_sms, s);
 }
