@@ -144,6 +144,7 @@ struct spg_plan {
   uint16_t* blk_cnt = nullptr;
   int blk_log2 = 12;
   int4* hcur = nullptr;
+  int32_t* hqueue = nullptr;  // next heavy row of the CTA kernels (zeroed before each launch)
   int window_bits = 1 << 20;  // heavy-path shape (heavy_shape)
   int heavy_threads = 1024;
 };
@@ -392,6 +393,7 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
   TRY(palloc(p, &p->f, n));
   TRY(palloc(p, &p->lo, n));
   TRY(palloc(p, &p->hi, n));
+  TRY(palloc(p, &p->hqueue, 1));
   {
     ProfScope ps(ctx, "plan/prepass", st);
     TRY_CUDA(launch_prepass(p->A, p->B, p->f, p->lo, p->hi, st), "prepass");
@@ -499,6 +501,7 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
     h.blk_off = p->blk_off;
     h.blk_cnt = p->blk_cnt;
     h.blk_log2 = p->blk_log2;
+    h.queue = p->hqueue;
     ProfScope ps(ctx, "sym/heavy", st);
     TRY_CUDA(launch_heavy(false, gram, h, p->heavy_threads, ctx->num_sms, st),
              "symbolic heavy");
@@ -660,6 +663,7 @@ spg_status execute_impl(spg_plan* p, spg_csr_out* C, cudaStream_t st) {
       h.sub_log2 = 31 - __builtin_clz((unsigned)h.cap);  // largest power of two <= cap
       if (h.sub_log2 > p->blk_log2) h.sub_log2 = p->blk_log2;
       h.hcur = p->hcur;
+      h.queue = p->hqueue;
       // rows fed by many short B rows stream through the warp kernel's
       // windows; rows dominated by long B rows, rows of more than 2^17
       // products, or all rows without block counts take the CTA kernel

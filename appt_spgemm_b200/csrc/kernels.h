@@ -213,6 +213,10 @@ struct HeavyArgs {
   // rows); split 0: all to the CTA kernel
   int64_t split;
   const int64_t* f;         // products per row (pre-pass)
+  // CTA kernels: a CTA takes its next row from this counter (launch_heavy
+  // zeroes it on the stream first), so a CTA that drew hub rows does not hold
+  // the others back
+  int32_t* queue;
 };
 
 // The heavy row goes to the windowed warp kernel: mean B-row length
