@@ -139,6 +139,15 @@ __device__ __forceinline__ long long block_sum64(long long v, long long* scratch
   return t;
 }
 
+// The CTA's next work item: one thread draws it from a counter that the
+// launcher zeroed; every thread of the CTA returns the same index.
+__device__ __forceinline__ int next_cta_item(int32_t* counter, int* s_next) {
+  __syncthreads();  // every thread has read the previous item
+  if (threadIdx.x == 0) *s_next = atomicAdd(counter, 1);
+  __syncthreads();
+  return *s_next;
+}
+
 // Block-wide exclusive scan of an int; returns this thread's prefix and sets
 // *total.  `scratch` holds 33 ints.  Contains two __syncthreads.
 __device__ __forceinline__ int block_exclusive_scan(int v, int* scratch, int* total) {

@@ -144,7 +144,7 @@ struct spg_plan {
   uint16_t* blk_cnt = nullptr;
   int blk_log2 = 12;
   int4* hcur = nullptr;
-  int32_t* hqueue = nullptr;  // next heavy row of the CTA kernels (zeroed before each launch)
+  int32_t* hqueue = nullptr;  // next row of the CTA-per-row kernels (zeroed before each launch)
   int window_bits = 1 << 20;  // heavy-path shape (heavy_shape)
   int heavy_threads = 1024;
 };
@@ -477,6 +477,7 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
   ra.rownnz = p->rownnz;
   ra.rowlow = p->rowlow;
   ra.status = ctx->d_status;
+  ra.queue = p->hqueue;
   ra.lo = p->lo;
   ra.hi = p->hi;
   int bins_used = 0;
@@ -622,6 +623,7 @@ spg_status execute_impl(spg_plan* p, spg_csr_out* C, cudaStream_t st) {
     ra.ccol = C->col;
     ra.cval = C->val;
     ra.status = ctx->d_status;
+    ra.queue = p->hqueue;
     ra.lo = p->lo;
     ra.hi = p->hi;
     ra.colbase = p->colbase;

@@ -29,18 +29,12 @@ size_t heavy_smem_bytes(bool numeric, int threads, int window_bits) {
   return b;
 }
 
-// The CTA's next row: one thread draws it from the launch's counter.  Rows
-// differ in cost by orders of magnitude (R-MAT hubs), so drawing them as CTAs
-// free up balances the SMs where dealing them out in turn did not (products
-// per CTA, max over mean: 1.20 at R-MAT 2^20, 1.50 at 2^18).  Numeric /
-// symbolic heavy time, dealt -> drawn: R-MAT 2^20 585 / 69.7 -> 493 / 57.1 ms,
-// 2^18 57.8 / 7.88 -> 46.3 / 5.49 ms, 2^16 11.4 / 1.21 -> 6.9 / 0.84 ms.
-__device__ __forceinline__ int next_heavy_row(int32_t* queue, int* s_next) {
-  __syncthreads();  // every thread has read the previous row
-  if (threadIdx.x == 0) *s_next = atomicAdd(queue, 1);
-  __syncthreads();
-  return *s_next;
-}
+// Rows are drawn from the launch's counter (next_cta_item) as CTAs free up.
+// Rows differ in cost by orders of magnitude (R-MAT hubs), and dealing them
+// out in turn left SMs idle (products per CTA, max over mean: 1.20 at R-MAT
+// 2^20, 1.50 at 2^18).  Numeric / symbolic heavy time, dealt -> drawn: R-MAT
+// 2^20 585 / 69.7 -> 493 / 57.1 ms, 2^18 57.8 / 7.88 -> 46.3 / 5.49 ms, 2^16
+// 11.4 / 1.21 -> 6.9 / 0.84 ms.
 
 // B rows at least this long are marked by the whole CTA, shorter ones by one
 // warp each.
@@ -109,7 +103,7 @@ __global__ void __launch_bounds__(1024, 2) k_heavy_sym(HeavyArgs h) {
   void* scratch = (void*)(st_long + blockDim.x);
   __shared__ int s_next;
   for (;;) {
-    const int r = next_heavy_row(h.queue, &s_next);
+    const int r = next_cta_item(h.queue, &s_next);
     if (r >= a.nrows) break;
     const int row = a.rows[r];
     const int lo = h.lo[row], hi = h.hi[row];
@@ -186,7 +180,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_heavy_num(HeavyArgs h) {
   const int tid = threadIdx.x;
   __shared__ int s_next;
   for (;;) {
-    const int r = next_heavy_row(h.queue, &s_next);
+    const int r = next_cta_item(h.queue, &s_next);
     if (r >= a.nrows) break;
     const int row = a.rows[r];
     const int hi = h.hi[row];

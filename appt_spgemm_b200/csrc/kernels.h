@@ -134,6 +134,9 @@ struct RowArgs {
   // batched plans: first column of the row's instance, subtracted from every
   // column index written (nullptr for a single matrix)
   const int32_t* colbase;
+  // CTA-per-row bins: rows are drawn from this counter (zeroed by the
+  // launcher) as CTAs free up; nullptr: dealt out in turn
+  int32_t* queue;
 };
 
 // Writes m sorted packed words ((col − lo) << LOG2T | slot) as a row's columns
