@@ -364,6 +364,7 @@ cudaError_t launch_heavy(bool numeric, bool gram, const HeavyArgs& h, int thread
                          cudaStream_t s) {
   if (h.r.nrows <= 0) return cudaSuccess;
   const size_t smem = heavy_smem_bytes(numeric, threads, h.window_bits);
+  if (!h.queue) return cudaErrorInvalidValue;  // the kernels draw their rows from it
   cudaError_t e = cudaMemsetAsync(h.queue, 0, sizeof(int32_t), s);
   if (e != cudaSuccess) return e;
   if (numeric && threads <= 512)
