@@ -189,7 +189,9 @@ spg_status spg_plan_get_info(const spg_plan* plan, spg_plan_info* info);
 /* Numeric phase + in-row sort (+ mirror for AAtS) into caller-owned buffers:
  * C->rowptr (n+1), C->col / C->val (info.nnz_c).  Asynchronous on `stream`.
  * A plan fixes the structure only: a plan may be executed again after A's
- * values (not its pattern) changed, and uses the current values. */
+ * values (not its pattern) changed, and uses the current values.  Executes of
+ * one plan must not overlap (they share the plan's workspace): order them on
+ * one stream, or synchronise between streams; separate plans run concurrently. */
 spg_status spg_execute(spg_plan* plan, spg_csr_out* C, void* stream);
 spg_status spg_plan_destroy(spg_plan* plan);
 
