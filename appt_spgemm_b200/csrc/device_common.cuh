@@ -148,6 +148,19 @@ __device__ __forceinline__ int next_cta_item(int32_t* counter, int* s_next) {
   return *s_next;
 }
 
+// The CTA's it-th work item of nitems.  A persistent launch (fewer CTAs than
+// items) draws items from the counter as CTAs free up, so costly items do not
+// pile up on a few CTAs.  A launch of a CTA per item takes item blockIdx.x and
+// retires after it: the hardware hands out the CTAs as SMs free up, and work
+// on a higher-priority stream gets the SMs in between (a CTA that kept drawing
+// would hold its SM until the last item).  Items past the end come back as
+// nitems.
+__device__ __forceinline__ int cta_item(int32_t* counter, int nitems, int it, int* s_next) {
+  if (counter && (int)gridDim.x < nitems) return next_cta_item(counter, s_next);
+  const long long r = (long long)blockIdx.x + (long long)it * gridDim.x;
+  return r < nitems ? (int)r : nitems;
+}
+
 // Block-wide exclusive scan of an int; returns this thread's prefix and sets
 // *total.  `scratch` holds 33 ints.  Contains two __syncthreads.
 __device__ __forceinline__ int block_exclusive_scan(int v, int* scratch, int* total) {

@@ -29,9 +29,9 @@ size_t heavy_smem_bytes(bool numeric, int threads, int window_bits) {
   return b;
 }
 
-// Rows are drawn from the launch's counter (next_cta_item) as CTAs free up.
-// Rows differ in cost by orders of magnitude (R-MAT hubs), and dealing them
-// out in turn left SMs idle (products per CTA, max over mean: 1.20 at R-MAT
+// In a persistent launch rows are drawn from the launch's counter as CTAs free
+// up (cta_item).  Rows differ in cost by orders of magnitude (R-MAT hubs), and
+// dealing them out in turn left SMs idle (products per CTA, max over mean: 1.20 at R-MAT
 // 2^20, 1.50 at 2^18).  Numeric / symbolic heavy time, dealt -> drawn: R-MAT
 // 2^20 585 / 69.7 -> 493 / 57.1 ms, 2^18 57.8 / 7.88 -> 46.3 / 5.49 ms, 2^16
 // 11.4 / 1.21 -> 6.9 / 0.84 ms.
@@ -102,8 +102,8 @@ __global__ void __launch_bounds__(1024, 2) k_heavy_sym(HeavyArgs h) {
   int* st_long = st_ex + blockDim.x;
   void* scratch = (void*)(st_long + blockDim.x);
   __shared__ int s_next;
-  for (;;) {
-    const int r = next_cta_item(h.queue, &s_next);
+  for (int it = 0;; ++it) {
+    const int r = cta_item(h.queue, a.nrows, it, &s_next);
     if (r >= a.nrows) break;
     const int row = a.rows[r];
     const int lo = h.lo[row], hi = h.hi[row];
@@ -179,8 +179,8 @@ __global__ void __launch_bounds__(MAXT, MINB) k_heavy_num(HeavyArgs h) {
   void* scratch = (void*)(st_long + HT);
   const int tid = threadIdx.x;
   __shared__ int s_next;
-  for (;;) {
-    const int r = next_cta_item(h.queue, &s_next);
+  for (int it = 0;; ++it) {
+    const int r = cta_item(h.queue, a.nrows, it, &s_next);
     if (r >= a.nrows) break;
     const int row = a.rows[r];
     const int hi = h.hi[row];

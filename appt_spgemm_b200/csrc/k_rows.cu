@@ -263,20 +263,15 @@ __global__ void __launch_bounds__(1024) k_hash_cta(RowArgs a) {
   void* scratch = (void*)(p + (size_t)G * 8);
   uint32_t* rtmp = (uint32_t*)(p + (size_t)G * 8 + kCtaScratchBytes);
   int* rcnt = (int*)(rtmp + T);
-  // rows drawn as CTAs free up (R-MAT 2^20 numeric 8192-slot bin 26.5 ->
-  // 25.2 ms, 4096-slot 8.5 -> 8.1 ms against dealing them out in turn)
-  if (a.queue) {
-    __shared__ int s_next;
-    for (;;) {
-      const int r = next_cta_item(a.queue, &s_next);
-      if (r >= a.nrows) break;
-      hash_row<LOG2T, NUMERIC, GRAM>(g, a, a.rows[r], keys, vals, st_bs, st_len, st_a, scratch,
-                                     rtmp, rcnt);
-    }
-  } else {
-    for (int r = blockIdx.x; r < a.nrows; r += gridDim.x)
-      hash_row<LOG2T, NUMERIC, GRAM>(g, a, a.rows[r], keys, vals, st_bs, st_len, st_a, scratch,
-                                     rtmp, rcnt);
+  // in a persistent launch rows are drawn as CTAs free up (R-MAT 2^20 numeric
+  // 8192-slot bin 26.5 -> 25.2 ms, 4096-slot 8.5 -> 8.1 ms against dealing
+  // them out in turn)
+  __shared__ int s_next;
+  for (int it = 0;; ++it) {
+    const int r = cta_item(a.queue, a.nrows, it, &s_next);
+    if (r >= a.nrows) break;
+    hash_row<LOG2T, NUMERIC, GRAM>(g, a, a.rows[r], keys, vals, st_bs, st_len, st_a, scratch,
+                                   rtmp, rcnt);
   }
 }
 
