@@ -134,8 +134,8 @@ struct RowArgs {
   // batched plans: first column of the row's instance, subtracted from every
   // column index written (nullptr for a single matrix)
   const int32_t* colbase;
-  // CTA-per-row bins: rows are drawn from this counter (zeroed by the
-  // launcher) as CTAs free up; nullptr: dealt out in turn
+  // CTA-per-row bins: in a persistent launch rows are drawn from this counter
+  // (zeroed by the launcher) as CTAs free up; nullptr: dealt out in turn
   int32_t* queue;
 };
 
@@ -216,9 +216,9 @@ struct HeavyArgs {
   // rows); split 0: all to the CTA kernel
   int64_t split;
   const int64_t* f;         // products per row (pre-pass)
-  // CTA kernels: a CTA takes its next row from this counter (launch_heavy
-  // zeroes it on the stream first), so a CTA that drew hub rows does not hold
-  // the others back
+  // CTA kernels: in a persistent launch (fewer CTAs than rows) a CTA takes its
+  // next row from this counter (launch_heavy zeroes it on the stream first),
+  // so a CTA that drew hub rows does not hold the others back; required
   int32_t* queue;
 };
 
