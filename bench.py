@@ -65,6 +65,9 @@ def parse_args():
                     help="requests per arrival rate in --mode serve")
     ap.add_argument("--serve-rates", default="50,500,5000")
     ap.add_argument("--serve-pool", type=int, default=40, help="distinct matrices in the pool")
+    ap.add_argument("--serve-seeds", type=int, default=1,
+                    help="arrival streams per rate in --mode serve (each run through both "
+                         "servers); figures are medians over the streams")
     return ap.parse_args()
 
 
@@ -517,14 +520,108 @@ def serve_pool(count, seed):
     return pool
 
 
-def run_serve(args):
+SERVE_FIGURES = ("p50_ms", "p99_ms", "small_p50_ms", "small_p99_ms", "sustained_gflops",
+                 "peak_reserved_gb")
+
+
+def aggregate_serve(runs):
+    """One (rate, server) entry from its runs over several arrival streams:
+    counts summed, each latency / throughput figure the median over the
+    streams, with its [min, max] under `<figure>_range` when there are two or
+    more."""
+    out = {"rate_per_s": runs[0]["rate_per_s"], "server": runs[0]["server"]}
+    for k in ("requests", "completed", "rejected", "failed", "batches", "small_requests"):
+        out[k] = sum(r[k] for r in runs)
+    for k in SERVE_FIGURES:
+        v = sorted(r[k] for r in runs if r[k] is not None)
+        if not v:
+            out[k] = None
+        elif len(v) % 2:
+            out[k] = v[len(v) // 2]
+        else:
+            out[k] = round((v[len(v) // 2 - 1] + v[len(v) // 2]) / 2, 3)
+        if len(runs) > 1:
+            out[k + "_range"] = [v[0], v[-1]] if v else None
+    out["streams"] = len(runs)
+    return out
+
+
+SERVERS = (("continuous_batching", dict(workers=4, batch_rows=65536, batch_max=64)),
+           ("queue_only", dict(workers=1, batch_rows=1, batch_max=1)))
+
+
+def serve_once(pool, ds, prods, rate, label, kw, picks, tasks, gaps):
+    """Run one arrival stream (request k: matrix picks[k], task tasks[k],
+    arriving gaps[k] after request k-1) through a server; the result entry."""
     import threading
 
-    import numpy as np
-    import torch
+    from appt_spgemm_b200 import _capi
+    from appt_spgemm_b200.engine import Server
 
-    from appt_spgemm_b200 import _capi, csr
-    from appt_spgemm_b200.engine import CsrDevice, Server
+    nreq = len(picks)
+    with Server(memory_budget_bytes=150 * 10**9, **kw) as srv:
+        ids = [None] * nreq
+        done = []
+
+        def consumer():
+            # release results in completion order: a request waiting for
+            # budget may need the memory of later ones
+            pending = set()
+            nxt = 0
+            while len(done) < nreq:
+                while nxt < nreq and ids[nxt] is not None:
+                    pending.add(nxt)
+                    nxt += 1
+                finished = []
+                for k in pending:
+                    info = srv.poll(ids[k])
+                    if info["status"] != _capi.SPG_ERR_NOT_READY:
+                        finished.append((k, info))
+                for k, info in finished:
+                    pending.discard(k)
+                    done.append((k, info))
+                    if info["status"] == _capi.SPG_OK:
+                        srv.release(ids[k])
+                if not finished:
+                    time.sleep(0.0002)
+
+        th = threading.Thread(target=consumer)
+        th.start()
+        start = time.perf_counter()
+        t_next = 0.0
+        for k in range(nreq):
+            t_next += gaps[k]
+            delay = start + t_next - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            ids[k] = srv.submit(ds[picks[k]], str(tasks[k]))
+        th.join()
+        st = srv.stats()
+    ok = [(k, i) for k, i in done if i["status"] == _capi.SPG_OK]
+    lat = sorted(i["done_ms"] - i["submit_ms"] for _, i in ok)
+    small = sorted(i["done_ms"] - i["submit_ms"] for k, i in ok
+                   if pool[int(picks[k])][0].n < 65536)
+
+    def pct(v, q):
+        return round(v[min(len(v) - 1, int(q * len(v)))], 3) if v else None
+    work = sum(2.0 * prods[(int(picks[k]), str(tasks[k]))] for k, _ in ok)
+    span_s = (max(i["done_ms"] for _, i in ok) - min(i["submit_ms"] for _, i in ok)) / 1e3 \
+        if ok else 0.0
+    return {"rate_per_s": rate, "server": label, "requests": nreq,
+            "completed": len(ok), "rejected": int(st["rejected"]),
+            "failed": int(st["failed"]), "batches": int(st["batches"]),
+            "p50_ms": pct(lat, 0.5), "p99_ms": pct(lat, 0.99),
+            "small_requests": len(small),
+            "small_p50_ms": pct(small, 0.5), "small_p99_ms": pct(small, 0.99),
+            "sustained_gflops": round(work / span_s / 1e9, 3) if ok and span_s > 0 else None,
+            "peak_reserved_gb": round(st["peak_reserved_bytes"] / 1e9, 2)}
+
+
+def run_serve(args):
+    import numpy as np
+
+    from appt_spgemm_b200 import csr
+    from appt_spgemm_b200.engine import CsrDevice
 
     t0 = time.time()
     pool = serve_pool(args.serve_pool, seed=5)
@@ -532,71 +629,21 @@ def run_serve(args):
     ds = [CsrDevice.from_host(A, "cuda:0") for A, _ in pool]
     prods = {(i, t): csr.products(A, "AA" if t == "AA" else "AAt")
              for i, (A, _) in enumerate(pool) for t in ("AA", "AAt")}
-    rng = np.random.Generator(np.random.PCG64(55))
-    results = []
-    for rate in [float(r) for r in args.serve_rates.split(",")]:
-        for label, kw in (("continuous_batching", dict(workers=4, batch_rows=65536, batch_max=64)),
-                          ("queue_only", dict(workers=1, batch_rows=1, batch_max=1))):
+    rates = [float(r) for r in args.serve_rates.split(",")]
+    runs = {}
+    for ri, rate in enumerate(rates):
+        for stream in range(args.serve_seeds):
+            # one arrival stream per (rate, stream), run through both servers
+            rng = np.random.Generator(np.random.PCG64([55, ri, stream]))
             nreq = args.serve_requests
             picks = rng.integers(0, len(pool), nreq)
             tasks = np.where(rng.random(nreq) < 0.5, "AA", "AAt")
             gaps = rng.exponential(1.0 / rate, nreq)
-            with Server(memory_budget_bytes=150 * 10**9, **kw) as srv:
-                ids = [None] * nreq
-                done = []
-
-                def consumer():
-                    # release results in completion order: a request waiting
-                    # for budget may need the memory of later ones
-                    pending = set()
-                    nxt = 0
-                    while len(done) < nreq:
-                        while nxt < nreq and ids[nxt] is not None:
-                            pending.add(nxt)
-                            nxt += 1
-                        finished = []
-                        for k in pending:
-                            info = srv.poll(ids[k])
-                            if info["status"] != _capi.SPG_ERR_NOT_READY:
-                                finished.append((k, info))
-                        for k, info in finished:
-                            pending.discard(k)
-                            done.append((k, info))
-                            if info["status"] == _capi.SPG_OK:
-                                srv.release(ids[k])
-                        if not finished:
-                            time.sleep(0.0002)
-
-                th = threading.Thread(target=consumer)
-                th.start()
-                start = time.perf_counter()
-                t_next = 0.0
-                for k in range(nreq):
-                    t_next += gaps[k]
-                    delay = start + t_next - time.perf_counter()
-                    if delay > 0:
-                        time.sleep(delay)
-                    ids[k] = srv.submit(ds[picks[k]], str(tasks[k]))
-                th.join()
-                st = srv.stats()
-            ok = [(k, i) for k, i in done if i["status"] == _capi.SPG_OK]
-            lat = sorted(i["done_ms"] - i["submit_ms"] for _, i in ok)
-            small = sorted(i["done_ms"] - i["submit_ms"] for k, i in ok
-                           if pool[int(picks[k])][0].n < 65536)
-
-            def pct(v, q):
-                return round(v[min(len(v) - 1, int(q * len(v)))], 3) if v else None
-            work = sum(2.0 * prods[(int(picks[k]), str(tasks[k]))] for k, _ in ok)
-            span_s = (max(i["done_ms"] for _, i in ok) - min(i["submit_ms"] for _, i in ok)) / 1e3
-            results.append({"rate_per_s": rate, "server": label, "requests": nreq,
-                            "completed": len(ok), "rejected": int(st["rejected"]),
-                            "failed": int(st["failed"]), "batches": int(st["batches"]),
-                            "p50_ms": pct(lat, 0.5), "p99_ms": pct(lat, 0.99),
-                            "small_requests": len(small),
-                            "small_p50_ms": pct(small, 0.5), "small_p99_ms": pct(small, 0.99),
-                            "sustained_gflops": round(work / span_s / 1e9, 3) if ok else None,
-                            "peak_reserved_gb": round(st["peak_reserved_bytes"] / 1e9, 2)})
-            print(json.dumps(results[-1]), file=sys.stderr, flush=True)
+            for label, kw in SERVERS:
+                r = serve_once(pool, ds, prods, rate, label, kw, picks, tasks, gaps)
+                runs.setdefault((rate, label), []).append(r)
+                print(json.dumps(dict(r, stream=stream)), file=sys.stderr, flush=True)
+    results = [aggregate_serve(runs[(rate, label)]) for rate in rates for label, _ in SERVERS]
     best = max((r["sustained_gflops"] or 0) for r in results)
     line = {"metric": "served GFLOP/s and p50/p99 latency, A·A / A·Aᵀ requests", "unit": "GFLOP/s",
             "mode": "serve", "value": best, "higher_is_better": True,
@@ -604,7 +651,8 @@ def run_serve(args):
             "config": {"workload": "Poisson arrivals; requests drawn uniformly from a pool of "
                                    f"{len(pool)} matrices (families 5-pt Laplacian / 27-pt stencil"
                                    " / R-MAT, n log-uniform [2k, 2M]); task A·A or A·Aᵀ 50/50; "
-                                   "budget 150 GB", "pool": [d for _, d in pool],
+                                   "budget 150 GB; each arrival stream runs through both servers",
+                       "streams_per_rate": args.serve_seeds, "pool": [d for _, d in pool],
                        "pool_generation_s": round(gen_s, 1)},
             "rates": results}
     print(json.dumps(line), flush=True)

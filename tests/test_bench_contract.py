@@ -45,3 +45,89 @@ def test_reference_arm_other_ranks_print_nothing():
     p = run_bench({"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"})
     assert p.returncode == 0, p.stderr[-2000:]
     assert p.stdout.strip() == ""
+
+
+def run_entry(rate, server, p50, gflops, small=None):
+    return {"rate_per_s": rate, "server": server, "requests": 10, "completed": 10,
+            "rejected": 0, "failed": 0, "batches": 1, "small_requests": 4,
+            "p50_ms": p50, "p99_ms": 2 * p50, "small_p50_ms": small, "small_p99_ms": small,
+            "sustained_gflops": gflops, "peak_reserved_gb": 1.0}
+
+
+def test_serve_aggregation_one_stream_is_that_stream():
+    import bench
+    r = run_entry(50.0, "queue_only", 120.0, 40.0, small=5.0)
+    a = bench.aggregate_serve([r])
+    for k, v in r.items():
+        assert a[k] == v, k
+    assert a["streams"] == 1 and "p50_ms_range" not in a
+
+
+def test_serve_aggregation_medians_ranges_and_sums():
+    import bench
+    runs = [run_entry(500.0, "continuous_batching", p, g, small=s)
+            for p, g, s in ((300.0, 50.0, None), (100.0, 70.0, 8.0), (200.0, 60.0, 2.0))]
+    a = bench.aggregate_serve(runs)
+    assert a["p50_ms"] == 200.0 and a["p50_ms_range"] == [100.0, 300.0]
+    assert a["sustained_gflops"] == 60.0 and a["sustained_gflops_range"] == [50.0, 70.0]
+    # a figure missing from a stream (no small requests there) is left out
+    assert a["small_p50_ms"] == 5.0 and a["small_p50_ms_range"] == [2.0, 8.0]
+    assert a["requests"] == 30 and a["completed"] == 30 and a["batches"] == 3
+    assert a["streams"] == 3
+    even = bench.aggregate_serve(runs[:2])
+    assert even["p50_ms"] == 200.0 and even["sustained_gflops"] == 60.0
+
+
+def test_serve_loop_runs_a_stream_through_a_server(monkeypatch):
+    """The serving loop's host side: every request is submitted at its arrival
+    time, polled to completion and released, and the entry counts them."""
+    import time
+    import types
+
+    import numpy as np
+
+    import bench
+    from appt_spgemm_b200 import _capi, engine
+
+    class FakeServer:
+        def __init__(self, memory_budget_bytes=0, workers=1, batch_rows=1, batch_max=1):
+            self.t0 = time.perf_counter()
+            self.submitted = {}
+            self.released = set()
+            FakeServer.last = self
+
+        def __enter__(self):
+            return self
+
+        def __exit__(self, *exc):
+            return False
+
+        def submit(self, A, task):
+            rid = len(self.submitted) + 1
+            self.submitted[rid] = ((time.perf_counter() - self.t0) * 1e3, task)
+            return rid
+
+        def poll(self, rid):
+            sub = self.submitted[rid][0]
+            return {"status": _capi.SPG_OK, "submit_ms": sub, "done_ms": sub + 1.0 + rid % 3}
+
+        def release(self, rid):
+            self.released.add(rid)
+
+        def stats(self):
+            return {"rejected": 0, "failed": 0, "batches": 0, "peak_reserved_bytes": 5e8}
+
+    monkeypatch.setattr(engine, "Server", FakeServer)
+    pool = [(types.SimpleNamespace(n=1000), "small"), (types.SimpleNamespace(n=100000), "large")]
+    prods = {(i, t): 1000 * (i + 1) for i in range(2) for t in ("AA", "AAt")}
+    picks = np.array([0, 1, 0, 1, 0])
+    tasks = np.array(["AA", "AAt", "AA", "AA", "AAt"])
+    gaps = np.full(5, 0.002)
+    r = bench.serve_once(pool, [None, None], prods, 500.0, "continuous_batching", {},
+                         picks, tasks, gaps)
+    assert r["requests"] == 5 and r["completed"] == 5 and r["small_requests"] == 3
+    assert r["rate_per_s"] == 500.0 and r["server"] == "continuous_batching"
+    assert FakeServer.last.released == {1, 2, 3, 4, 5}
+    assert [t for _, t in FakeServer.last.submitted.values()] == list(tasks)
+    assert r["p50_ms"] >= 1.0 and r["sustained_gflops"] > 0
+    assert r["peak_reserved_gb"] == 0.5
