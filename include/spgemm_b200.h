@@ -181,8 +181,10 @@ spg_status spg_destroy(spg_ctx* ctx);
 spg_status spg_check_device_status(spg_ctx* ctx, void* stream);
 
 /* ---- plan / execute (replaces the sizing half of run_ours) ---------------- */
-/* Pre-pass + binning + symbolic phase.  One pinned readback (nnz(C)) is the
- * only host synchronisation.  A must stay valid until the plan is destroyed. */
+/* Pre-pass + binning + symbolic phase.  Three host synchronisations, each a
+ * small pinned readback: the validity verdict on A, the bin sizes, nnz(C).
+ * When it returns, no kernel of the plan's symbolic phase is still running.
+ * A must stay valid until the plan is destroyed. */
 spg_status spg_plan_create(spg_ctx* ctx, spg_task task, const spg_csr_dev* A,
                            void* stream, spg_plan** plan);
 spg_status spg_plan_get_info(const spg_plan* plan, spg_plan_info* info);
