@@ -136,3 +136,64 @@ def test_er_and_banded_shapes():
     rows = np.repeat(np.arange(Bd.n), np.diff(Bd.rowptr))
     assert np.abs(rows - Bd.col).max() <= 16
     assert (rows == Bd.col).sum() == 3000
+
+
+def declared_prototypes():
+    """name -> number of parameters, from the header's prototypes."""
+    text = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    out = {}
+    for m in re.finditer(r"\b(spg_[a-z0-9_]+)\s*\(([^;{}]*?)\)\s*;", text):
+        params = m.group(2).strip()
+        out[m.group(1)] = 0 if params in ("", "void") else params.count(",") + 1
+    return out
+
+
+def test_binding_argument_counts_match_the_header():
+    protos = declared_prototypes()
+    assert set(protos) == set(declared_functions())
+    wrong = {n: (k, len(_capi.SIGNATURES[n][1])) for n, k in protos.items()
+             if len(_capi.SIGNATURES[n][1]) != k}
+    assert not wrong, wrong
+
+
+STRUCTS = {"spg_csr_dev": "SpgCsrDev", "spg_csr_out": "SpgCsrOut", "spg_config": "SpgConfig",
+           "spg_eng_result": "SpgEngResult", "spg_plan_info": "SpgPlanInfo",
+           "spg_descriptors": "SpgDescriptors", "spg_server_config": "SpgServerConfig",
+           "spg_request_info": "SpgRequestInfo", "spg_server_stats": "SpgServerStats",
+           "spg_host_csr": "SpgHostCsr"}
+
+
+def c_field_name(field):
+    """The C name of a mirrored field: Python keywords carry a trailing '_'."""
+    import keyword
+    return field[:-1] if field.endswith("_") and keyword.iskeyword(field[:-1]) else field
+
+
+def test_binding_structs_have_the_c_layout(tmp_path):
+    """Size and every field offset of each ctypes mirror equal the C struct's,
+    as gcc lays it out from the header."""
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc not available")
+    lines = ["#include <stdio.h>", "#include <stddef.h>", f'#include "{HEADER}"',
+             "int main(void) {"]
+    for cname, pyname in STRUCTS.items():
+        cls = getattr(_capi, pyname)
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for field, _ in cls._fields_:
+            cfield = c_field_name(field)
+            lines.append(f'  printf("{cname} {field} %zu\\n", offsetof({cname}, {cfield}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+    for line in out.splitlines():
+        cname, what, value = line.split()
+        cls = getattr(_capi, STRUCTS[cname])
+        got = ctypes.sizeof(cls) if what == "size" else getattr(cls, what).offset
+        assert got == int(value), (cname, what, got, value)
+    # every C field is mirrored (the C program only names mirrored fields, so
+    # a C field missing from the mirror shows up as a size difference above)
