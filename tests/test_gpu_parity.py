@@ -15,6 +15,7 @@ import pytest
 import oracle
 from appt_spgemm_b200 import _capi, csr
 from appt_spgemm_b200._capi import SpgemmError
+from parity import assert_same_csr
 
 pytestmark = pytest.mark.gpu
 
@@ -38,13 +39,7 @@ def dev(A):
 
 
 def assert_same(C, ref, label):
-    rp, ci, cx = C.to_host()
-    orp, oci, ocx = ref
-    assert rp.shape == orp.shape, label
-    assert np.array_equal(rp, orp), f"{label}: rowptr"
-    assert np.array_equal(ci, oci), f"{label}: col"
-    assert np.array_equal(cx.view(np.int64), ocx.view(np.int64)), (
-        f"{label}: values, max |diff| {np.abs(cx - ocx).max() if len(cx) else 0}")
+    assert_same_csr(C.to_host(), ref, label)
 
 
 def run_case(eng, A, task, label):
