@@ -52,10 +52,14 @@ def parse_args():
                     help="skip the CPU oracle, cuSPARSE and reference-GPU baselines")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="CPU work of the oracle baseline sample")
-    ap.add_argument("--mode", choices=["plain", "rmat", "batch", "serve"], default="plain",
+    ap.add_argument("--mode", choices=["plain", "rmat", "laplace", "batch", "serve"],
+                    default="plain",
                     help="plain: the headline stencil benchmark; rmat: the power-law graph "
-                         "(R-MAT 2^20, heavy rows); batch: 512 matrices in one batched product "
-                         "vs back-to-back calls; serve: Poisson request stream")
+                         "(R-MAT 2^20, heavy rows); laplace: the 2-D 5-point Laplacian "
+                         "(64^2, launch-latency-bound: µs per call); batch: 512 matrices in one "
+                         "batched product vs back-to-back calls; serve: Poisson request stream")
+    ap.add_argument("--laplace-side", type=int, default=64,
+                    help="grid side of --mode laplace")
     ap.add_argument("--rmat-scale", type=int, default=20, help="R-MAT scale of --mode rmat")
     ap.add_argument("--er-degree", type=float, default=0.0,
                     help="--mode rmat on an Erdős–Rényi graph of n = 2^scale with this mean "
@@ -307,8 +311,27 @@ def reference_gpu_baseline(A, p_aa, p_aat):
 
 
 # ---------------------------------------------------------------------------
-# power-law graph: R-MAT 2^20 (edge factor 16, (.57,.19,.19,.05), seed 3)
+# single matrices timed per call: the power-law graph R-MAT 2^20 (edge factor
+# 16, (.57,.19,.19,.05), seed 3), an Erdős–Rényi graph, or the 2-D 5-point
+# Laplacian 64^2
 # ---------------------------------------------------------------------------
+def single_matrix(args):
+    """The matrix of --mode rmat / laplace: (A, description, metric label)."""
+    from appt_spgemm_b200 import csr
+    if args.mode == "laplace":
+        A = csr.laplace2d(args.laplace_side)
+        return A, (f"2-D 5-point Laplacian {args.laplace_side}^2 (n={A.n}, nnz={A.nnz}), 4.0 "
+                   "diagonal, -1.0 neighbours"), "2-D 5-point Laplacian"
+    if args.er_degree > 0:
+        A = csr.erdos_renyi(1 << args.rmat_scale, args.er_degree, seed=3)
+        return A, (f"Erdős–Rényi n=2^{args.rmat_scale} (n={A.n}, nnz={A.nnz}), mean degree "
+                   f"{args.er_degree:g}, seed 3"), "random graph"
+    A = csr.rmat(args.rmat_scale, 16, seed=3)
+    return A, (f"R-MAT scale {args.rmat_scale} (n={A.n}, nnz={A.nnz}), edge factor 16, "
+               "(a,b,c,d)=(.57,.19,.19,.05), seed 3, duplicates merged, self-loops kept, "
+               "values uniform(0,1)"), "power-law graph"
+
+
 def run_rmat(args):
     import torch
 
@@ -316,15 +339,7 @@ def run_rmat(args):
     from appt_spgemm_b200.engine import CsrDevice, Engine
 
     t0 = time.time()
-    if args.er_degree > 0:
-        A = csr.erdos_renyi(1 << args.rmat_scale, args.er_degree, seed=3)
-        graph = (f"Erdős–Rényi n=2^{args.rmat_scale} (n={A.n}, nnz={A.nnz}), mean degree "
-                 f"{args.er_degree:g}, seed 3")
-    else:
-        A = csr.rmat(args.rmat_scale, 16, seed=3)
-        graph = (f"R-MAT scale {args.rmat_scale} (n={A.n}, nnz={A.nnz}), edge factor 16, "
-                 "(a,b,c,d)=(.57,.19,.19,.05), seed 3, duplicates merged, self-loops kept, "
-                 "values uniform(0,1)")
+    A, graph, label = single_matrix(args)
     gen_s = time.time() - t0
     prods = {"AA": csr.products(A, "AA"), "AAt": csr.products(A, "AAt")}
     n, nnz = A.n, A.nnz
@@ -359,6 +374,7 @@ def run_rmat(args):
             ms = statistics.median(ts)
             alg = 4 * (n + 1) + 12 * nnz + 8 * (n + 1) + 12 * info["nnz_c"]
             tasks[task] = {"ms_median": round(ms, 3), "ms_mean": round(statistics.mean(ts), 3),
+                           "us_per_call": round(ms * 1e3, 1),
                            "gflops": round(2.0 * prods[task] / (ms * 1e-3) / 1e9, 3),
                            "products": prods[task], "nnz_c": info["nnz_c"],
                            "heavy_rows": info["heavy_rows"],
@@ -370,14 +386,15 @@ def run_rmat(args):
     total_ms = tasks["AA"]["ms_median"] + tasks["AAt"]["ms_median"]
     value = 2.0 * (prods["AA"] + prods["AAt"]) / (total_ms * 1e-3) / 1e9
     top_label, top_ms = max(kernels["AA"].items(), key=lambda kv: kv[1])
-    line = {"metric": "GFLOP/s (2×intermediate products/s) A·A & A·Aᵀ, "
-                      + ("random graph" if args.er_degree > 0 else "power-law graph"),
-            "value": round(value, 3), "unit": "GFLOP/s", "mode": "rmat", "n_gpus": 1,
+    line = {"metric": "GFLOP/s (2×intermediate products/s) A·A & A·Aᵀ, " + label,
+            "value": round(value, 3), "unit": "GFLOP/s", "mode": args.mode, "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total_ms, 3),
             "higher_is_better": True, "dtype": "f64", "data": "synthetic (seeded generator)",
             "config": {"workload": graph + "; one step = A·A + A·Aᵀ",
                        "generation_s": round(gen_s, 1),
-                       "l2": "C exceeds L2 by far; no flush needed"},
+                       "l2": ("inputs and C fit in L2: warm-cache calls, launch-latency-bound"
+                              if args.mode == "laplace" else
+                              "C exceeds L2 by far; no flush needed")},
             "tasks": tasks, "kernels_ms_per_call": kernels,
             "roofline": {"bound": "hbm", "kernel": "whole call (A·A)",
                          "achieved": round(tasks["AA"]["alg_bytes"] /
@@ -688,7 +705,7 @@ def main():
     if args.impl == "reference":
         run_reference(args)
         return
-    if args.mode == "rmat":
+    if args.mode in ("rmat", "laplace"):
         run_rmat(args)
         return
     if args.mode == "batch":

@@ -131,3 +131,24 @@ def test_serve_loop_runs_a_stream_through_a_server(monkeypatch):
     assert [t for _, t in FakeServer.last.submitted.values()] == list(tasks)
     assert r["p50_ms"] >= 1.0 and r["sustained_gflops"] > 0
     assert r["peak_reserved_gb"] == 0.5
+
+
+def test_single_matrix_workloads():
+    """The matrices of --mode laplace / rmat: the 5-point Laplacian 64² of the
+    small plain configuration (n 4,096, nnz 20,224, 100,104 products), R-MAT and
+    Erdős–Rényi at the requested scale."""
+    import types
+
+    import bench
+    from appt_spgemm_b200 import csr
+
+    args = types.SimpleNamespace(mode="laplace", laplace_side=64, rmat_scale=10, er_degree=0.0)
+    A, desc, label = bench.single_matrix(args)
+    assert (A.n, A.nnz) == (4096, 20224) and csr.products(A, "AA") == 100104
+    assert "Laplacian" in desc and label == "2-D 5-point Laplacian"
+    args.mode = "rmat"
+    A, desc, label = bench.single_matrix(args)
+    assert A.n == 1024 and label == "power-law graph" and "R-MAT scale 10" in desc
+    args.er_degree = 8.0
+    A, desc, label = bench.single_matrix(args)
+    assert A.n == 1024 and label == "random graph"
