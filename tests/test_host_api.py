@@ -197,3 +197,18 @@ def test_binding_structs_have_the_c_layout(tmp_path):
         assert got == int(value), (cname, what, got, value)
     # every C field is mirrored (the C program only names mirrored fields, so
     # a C field missing from the mirror shows up as a size difference above)
+
+
+def test_cli_errors_before_the_device(golden_dir, tmp_path):
+    """The CLI's argument and input errors: one line on stderr, exit 1, found
+    before any device work (so they hold on a machine without a GPU)."""
+    import subprocess
+    cli = os.path.join(os.path.dirname(_capi.LIB_PATH), "spgemm_b200_cli")
+    lap = os.path.join(golden_dir, "laplace2d_64.csr")
+    p = subprocess.run([cli], capture_output=True, text=True)
+    assert p.returncode == 1 and p.stderr.startswith("usage:")
+    p = subprocess.run([cli, "t", lap, "AtA"], capture_output=True, text=True)
+    assert p.returncode == 1 and "task must be AA, AAt or AAtS" in p.stderr and not p.stdout
+    p = subprocess.run([cli, "t", str(tmp_path / "missing.csr"), "AA"], capture_output=True,
+                       text=True)
+    assert p.returncode == 1 and p.stderr.startswith("spgemm_b200: read:") and not p.stdout
