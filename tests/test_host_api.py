@@ -212,3 +212,22 @@ def test_cli_errors_before_the_device(golden_dir, tmp_path):
     p = subprocess.run([cli, "t", str(tmp_path / "missing.csr"), "AA"], capture_output=True,
                        text=True)
     assert p.returncode == 1 and p.stderr.startswith("spgemm_b200: read:") and not p.stdout
+
+
+def test_no_gpu_means_errors_not_a_cpu_fallback():
+    """Without a usable CUDA device every product entry point fails loudly —
+    a status from the C ABI, an exception from Python — and nothing is
+    computed on the host instead."""
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    from appt_spgemm_b200.engine import Engine
+    L = _capi.lib()
+    ctx = ctypes.c_void_p()
+    assert L.spg_create(ctypes.byref(ctx), None) == _capi.SPG_ERR_CUDA
+    assert not ctx.value
+    r = _capi.SpgEngResult()
+    assert L.spg_run_ours(b"AA", None, None, None, 0, 0, 1, ctypes.byref(r)) == _capi.SPG_ERR_CUDA
+    assert b"cuda" in L.spg_last_error_string().lower()
+    with pytest.raises(RuntimeError):
+        Engine("cuda:0")
