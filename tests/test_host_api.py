@@ -203,7 +203,7 @@ def test_cli_errors_before_the_device(golden_dir, tmp_path):
     """The CLI's argument and input errors: one line on stderr, exit 1, found
     before any device work (so they hold on a machine without a GPU)."""
     import subprocess
-    cli = os.path.join(os.path.dirname(_capi.LIB_PATH), "spgemm_b200_cli")
+    cli = _capi.CLI_PATH
     lap = os.path.join(golden_dir, "laplace2d_64.csr")
     p = subprocess.run([cli], capture_output=True, text=True)
     assert p.returncode == 1 and p.stderr.startswith("usage:")
