@@ -286,7 +286,10 @@ spg_status spg_server_copy_result(spg_server* s, uint64_t id, int64_t* rowptr, i
 /* Drop a finished result: frees its device memory and returns its budget. */
 spg_status spg_server_release(spg_server* s, uint64_t id);
 spg_status spg_server_stats_get(spg_server* s, spg_server_stats* st);
-/* Waits for in-flight requests, frees all results, stops the workers. */
+/* Stops the workers: requests running on the device finish; a request that
+ * would still have to wait for budget ends with an error status instead of
+ * running.  Then frees all results.  The server's functions may be called
+ * from several host threads; destroy is the last call. */
 spg_status spg_server_destroy(spg_server* s);
 
 /* plan + execute with C allocated from the context pool; C->nnz is set. */
