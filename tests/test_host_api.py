@@ -231,3 +231,28 @@ def test_no_gpu_means_errors_not_a_cpu_fallback():
     assert b"cuda" in L.spg_last_error_string().lower()
     with pytest.raises(RuntimeError):
         Engine("cuda:0")
+
+
+def test_batch_mix_follows_its_recipe():
+    """The batched workload's generator: n log-uniform in [1k, 64k), banded and
+    Erdős–Rényi matrices alternating, their parameters in range, values in
+    [−1, 1), valid CSR, and the same seed gives the same matrices."""
+    mats, params = csr.batch_mix(64, seed=4)
+    assert len(mats) == len(params) == 64
+    for b, (A, p) in enumerate(zip(mats, params)):
+        A.validate()
+        assert A.n == p["n"] and 1000 <= A.n < 64000
+        assert p["kind"] == ("banded" if b % 2 == 0 else "er")
+        if p["kind"] == "banded":
+            assert 3 <= p["bw"] <= 64
+            rows = np.repeat(np.arange(A.n), np.diff(A.rowptr))
+            assert np.abs(rows - A.col).max() <= p["bw"]
+            assert (rows == A.col).sum() == A.n  # diagonal always present
+        else:
+            assert 4.0 <= p["lambda"] < 32.0
+        assert A.val.min() >= -1.0 and A.val.max() < 1.0
+    ns = np.array([p["n"] for p in params])
+    assert ns.min() < 4000 and ns.max() > 16000  # spread over the log range
+    again, _ = csr.batch_mix(8, seed=4)
+    for A, B in zip(mats[:8], again):
+        assert np.array_equal(A.col, B.col) and np.array_equal(A.val, B.val)
