@@ -152,3 +152,25 @@ def test_single_matrix_workloads():
     args.er_degree = 8.0
     A, desc, label = bench.single_matrix(args)
     assert A.n == 1024 and label == "random graph"
+
+
+def test_serve_pool_follows_its_recipe():
+    """The serving pool: each matrix one of the three families, its size from
+    n log-uniform in [2k, 2M] rounded to the family's shape (grid side or
+    R-MAT scale), and the pool fixed by its seed."""
+    import re
+
+    import bench
+    pool = bench.serve_pool(12, seed=5)
+    assert len(pool) == 12
+    for A, desc in pool:
+        A.validate()
+        m = re.fullmatch(r"(laplace2d|stencil27|rmat) (\d+)\^(\d+)", desc)
+        assert m, desc
+        fam, base, exp = m.group(1), int(m.group(2)), int(m.group(3))
+        assert A.n == base ** exp
+        assert 2000 <= A.n <= 2 ** 21  # rounding of the side or scale can pass 2M a little
+        assert (fam == "rmat") == (base == 2)
+    first = bench.serve_pool(3, seed=5)
+    assert [d for _, d in first] == [d for _, d in pool[:3]]
+    assert all(a.nnz == b.nnz for (a, _), (b, _) in zip(first, pool))
