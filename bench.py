@@ -16,6 +16,13 @@ is needed between steps.
 Multi-GPU: the product has no exchange step, so N GPUs run N independent
 replicas (weak scaling); the time is the max over ranks.  --impl reference
 times the CPU oracle (the reference's algorithm, restated) on the host cores.
+
+Other workloads, one GPU each: --mode rmat (R-MAT 2^20, heavy rows; or an
+Erdős–Rényi graph with --er-degree), --mode laplace (the 2-D 5-point
+Laplacian 64², microseconds per call), --mode batch (512 matrices in one
+batched product and in graph replay against back-to-back calls), --mode serve
+(Poisson request streams through the request server and a one-worker queue;
+--serve-seeds repeats each rate over several streams).
 """
 import argparse
 import json
