@@ -42,6 +42,7 @@ SEED = 2
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 TRAFFIC = os.path.join(ROOT, "profiles", "ncu_traffic.json")
 FALLBACK_HBM_GBS = 6650.0
+METRIC = "GFLOP/s (2×intermediate products/s) A·A & A·Aᵀ"
 
 
 def parse_args():
@@ -57,6 +58,9 @@ def parse_args():
                          "also timed beside the line)")
     ap.add_argument("--no-baselines", action="store_true",
                     help="skip the CPU oracle, cuSPARSE and reference-GPU baselines")
+    ap.add_argument("--no-sub", action="store_true",
+                    help="skip the sub-results of the default line (the 5-point Laplacian 64^2 "
+                         "per call and the 512-matrix batch)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="CPU work of the oracle baseline sample")
     ap.add_argument("--mode", choices=["plain", "rmat", "laplace", "batch", "serve"],
@@ -215,40 +219,36 @@ def cpu_oracle_rate(A, seconds, nthreads, label_rows=None):
 
 def run_reference(args):
     """--impl reference: the reference's algorithm on the host cores (the CPU
-    oracle restating it, all threads), same workload, metric and config; each
-    step is a bounded sample of rows of both products."""
+    oracle restating it, all threads), same workload, metric and config.  Each
+    step computes every row of A·A and of A·Aᵀ.  This arm loads no engine code:
+    the stencil comes from the oracle's own generator (byte-identical to the
+    engine's) and Aᵀ from the oracle's transpose."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     import oracle
-    A, p_aa, p_aat = workload(args.side)
+    A = oracle.gen_stencil27(args.side, SEED)
+    B_t = oracle.transpose(A)
     nthreads = os.cpu_count() or 1
-    B_t = A.transpose()
     f_aa, f_aat = row_products(A, A), row_products(A, B_t)
-    # size one step to about 4 s of work: calibrate on a small block
-    t0 = time.perf_counter()
-    oracle.rows_stream(A, A, 0, 512, nthreads)
-    rate_rows = 512 / max(time.perf_counter() - t0, 1e-6)
-    rows = int(min(A.n, max(512, rate_rows * 2.0)))
-    times, prods = [], []
+    prods = int(f_aa.sum() + f_aat.sum())
+    times = []
     for step in range(args.warmup + args.steps):
-        r0 = (step * rows) % max(1, A.n - rows + 1)
         t0 = time.perf_counter()
-        oracle.rows_stream(A, A, r0, r0 + rows, nthreads)
-        oracle.rows_stream(A, B_t, r0, r0 + rows, nthreads)
+        oracle.rows_stream(A, A, 0, A.n, nthreads)
+        oracle.rows_stream(A, B_t, 0, A.n, nthreads)
         dt = time.perf_counter() - t0
         if step >= args.warmup:
             times.append(dt)
-            prods.append(int(f_aa[r0:r0 + rows].sum() + f_aat[r0:r0 + rows].sum()))
-    gflops = 2.0 * sum(prods) / sum(times) / 1e9
-    sample = (f"{rows} consecutive rows of A·A and of A·Aᵀ per step "
-              f"({100.0 * rows / A.n:.2f}% of the rows)")
-    line = {"metric": "GFLOP/s (2×intermediate products/s) A·A & A·Aᵀ", "value": round(gflops, 3),
+    gflops = 2.0 * prods * len(times) / sum(times) / 1e9
+    sample = (f"every row of A·A and of A·Aᵀ each step ({A.n} rows, {prods} products per "
+              f"step, {nthreads} threads)")
+    line = {"metric": METRIC, "value": round(gflops, 3),
             "unit": "GFLOP/s", "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(1e3 * statistics.mean(times), 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded generator)",
-            "config": config(args, A, {"device": "host CPU"}),
+            "config": config(args, A),
             "cpu_baseline": {"value": round(gflops, 3), "unit": "GFLOP/s", "cores": nthreads,
                              "kind": "port", "sample": sample},
             "e2e": {"value": round(gflops, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": 0,
@@ -259,7 +259,7 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # GPU baselines outside the timed region: cuSPARSE, the reference's CUDA engine
 # ---------------------------------------------------------------------------
-def cusparse_baseline(dA, A, p_aa, p_aat):
+def cusparse_baseline(dA, A, p_aa, p_aat, reps=5):
     import ctypes
 
     from appt_spgemm_b200 import _capi
@@ -279,7 +279,7 @@ def cusparse_baseline(dA, A, p_aa, p_aat):
         nnz = ctypes.c_longlong()
         chk = (ctypes.c_double * 3)()
         err = ctypes.create_string_buffer(256)
-        rc = fn(tid, dA.rowptr.data_ptr(), dA.col.data_ptr(), dA.val.data_ptr(), A.n, A.nnz, 5, 2,
+        rc = fn(tid, dA.rowptr.data_ptr(), dA.col.data_ptr(), dA.val.data_ptr(), A.n, A.nnz, reps, 2,
                 ctypes.byref(mean), ctypes.byref(mn), ctypes.byref(nnz), chk, err, 256)
         if rc != 0:
             out[task] = {"error": err.value.decode()}
@@ -290,9 +290,10 @@ def cusparse_baseline(dA, A, p_aa, p_aat):
     return out
 
 
-def reference_gpu_baseline(A, p_aa, p_aat):
+def reference_gpu_baseline(A, p_aa, p_aat, reps=5):
     """The reference's own CUDA engine (src/spgemm.cu built unmodified for sm_80,
-    JIT-run on the B200) on a CSR1 file of the same matrix, reps=5."""
+    JIT-run on the B200) on a CSR1 file of the same matrix, `reps` timed calls
+    (its RESULT line reports their mean)."""
     exe = os.path.join(ROOT, "oracle", "_ref", "spgemm_ref")
     if not os.path.exists(exe):
         return {"error": "reference engine binary not built"}
@@ -303,7 +304,7 @@ def reference_gpu_baseline(A, p_aa, p_aat):
         csr.write_bin(A, path)
         for task, prods in (("AA", p_aa), ("AAt", p_aat), ("AAtS", p_aat)):
             try:
-                r = subprocess.run([exe, "bench", path, task, "5"], capture_output=True, text=True,
+                r = subprocess.run([exe, "bench", path, task, str(reps)], capture_output=True, text=True,
                                    timeout=300)
                 res = [ln.split(",") for ln in r.stdout.splitlines() if ln.startswith("RESULT,")]
                 if r.returncode != 0 or not res:
@@ -683,6 +684,127 @@ def run_serve(args):
 
 
 # ---------------------------------------------------------------------------
+# sub-results of the default line: the other configurations that fit one GPU
+# ---------------------------------------------------------------------------
+def time_calls(fn, reps, warm=3):
+    """CUDA-event times (ms) of `reps` calls of fn() on the current stream, after
+    `warm` untimed ones; a synchronize on both sides of each call."""
+    import torch
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    out = []
+    for _ in range(reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        torch.cuda.synchronize()
+        out.append(a.elapsed_time(b))
+    return out
+
+
+def ms_summary(ts):
+    return {"ms_median": round(statistics.median(ts), 4), "ms_mean": round(statistics.mean(ts), 4),
+            "ms_min": round(min(ts), 4), "calls": len(ts)}
+
+
+def laplace_subresult(eng, reps=50):
+    """The 2-D 5-point Laplacian 64² (n = 4,096, 4.0 diagonal, −1.0 neighbours):
+    full calls (plan + execute) of A·A and A·Aᵀ in µs, beside cuSPARSE and the
+    reference's CUDA engine on the same matrix; launch-latency-bound."""
+    from appt_spgemm_b200 import csr
+    from appt_spgemm_b200.engine import CsrDevice
+    A = csr.laplace2d(64)
+    dA = CsrDevice.from_host(A, "cuda:0")
+    prods = {"AA": csr.products(A, "AA"), "AAt": csr.products(A, "AAt")}
+    out = {"workload": f"2-D 5-point Laplacian 64^2 (n={A.n}, nnz={A.nnz}), one full call "
+                       "(plan + execute) per product", "products": prods, "ours": {}}
+    for task in ("AA", "AAt"):
+        ts = time_calls(lambda: eng.multiply(dA, task), reps)
+        m = ms_summary(ts)
+        m["us_per_call"] = round(1e3 * m["ms_median"], 1)
+        m["gflops"] = round(2.0 * prods[task] / (m["ms_median"] * 1e-3) / 1e9, 3)
+        pl = eng.plan(dA, task)
+        m["nnz_c"] = pl.nnz_c
+        pl.close()
+        out["ours"][task] = m
+    out["cusparse"] = cusparse_baseline(dA, A, prods["AA"], prods["AAt"], reps=20)
+    out["reference_gpu_engine"] = reference_gpu_baseline(A, prods["AA"], prods["AAt"], reps=20)
+    for k in ("cusparse", "reference_gpu_engine"):
+        for task in ("AA", "AAt"):
+            r = out[k].get(task, {})
+            if "ms_mean" in r:
+                r["us_per_call"] = round(1e3 * r.get("ms_min", r["ms_mean"]), 1)
+    return out
+
+
+def batch_subresult(eng, reps=3):
+    """512 matrices (n log-uniform [1k, 64k]; half random banded, half
+    Erdős–Rényi), A·A of each, with the same work on both sides of each ratio:
+    one batched plan + execute against 512 full calls, and one graph replay of
+    the batched execute against 512 graph replays of per-instance executes."""
+    import torch
+
+    from appt_spgemm_b200 import csr
+    from appt_spgemm_b200.engine import CsrDevice
+    t0 = time.time()
+    mats, _ = csr.batch_mix(512, seed=4)
+    gen_s = time.time() - t0
+    prods = sum(csr.products(A, "AA") for A in mats)
+    ds = [CsrDevice.from_host(A, "cuda:0") for A in mats]
+    gf = lambda ms: round(2.0 * prods / (ms * 1e-3) / 1e9, 3)  # noqa: E731
+
+    def back_to_back():
+        for d in ds:
+            eng.multiply(d, "AA")
+
+    full_each = statistics.median(time_calls(back_to_back, reps, warm=1))
+    full_batched = statistics.median(time_calls(lambda: eng.multiply_batched(ds, "AA"), reps,
+                                                warm=1))
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        plans = [eng.plan(d, "AA", stream=side) for d in ds]
+        outs = [p.execute(stream=side) for p in plans]
+        graphs = [p.capture_graph(o, side) for p, o in zip(plans, outs)]
+        bp = eng.plan_batched(ds, "AA", stream=side)
+        bout = bp.execute(stream=side)
+        bg = bp.capture_graph(bout, side)
+    side.synchronize()
+
+    def replay_each():
+        for g in graphs:
+            g.launch(side)
+        torch.cuda.current_stream().wait_stream(side)
+
+    def replay_batched():
+        bg.launch(side)
+        torch.cuda.current_stream().wait_stream(side)
+
+    rep_each = statistics.median(time_calls(replay_each, reps, warm=1))
+    rep_batched = statistics.median(time_calls(replay_batched, reps, warm=1))
+    for g in graphs + [bg]:
+        g.close()
+    for p in plans + [bp]:
+        p.close()
+    return {"workload": "512 matrices, n log-uniform [1k, 64k], half banded (bw U{3..64}, 30% "
+                        "fill), half Erdős–Rényi (λ U(4,32)), A·A of each",
+            "total_nnz": int(sum(A.nnz for A in mats)), "total_products": int(prods),
+            "generation_s": round(gen_s, 1),
+            "full_calls": {"back_to_back_ms": round(full_each, 3), "batched_ms": round(full_batched, 3),
+                           "back_to_back_gflops": gf(full_each), "batched_gflops": gf(full_batched),
+                           "speedup": round(full_each / full_batched, 2),
+                           "note": "plan + execute on both sides"},
+            "graph_replay": {"per_instance_ms": round(rep_each, 3),
+                             "batched_ms": round(rep_batched, 3),
+                             "per_instance_gflops": gf(rep_each), "batched_gflops": gf(rep_batched),
+                             "speedup": round(rep_each / rep_batched, 2),
+                             "note": "execute phase of reused plans, replayed as CUDA graphs on "
+                                     "both sides"},
+            "batched_replay_vs_back_to_back_calls": round(full_each / rep_batched, 2)}
+
+
+# ---------------------------------------------------------------------------
 # replicas: every rank runs the whole workload; the job's step time is the
 # slowest rank's, its throughput the sum of the replicas' work over that time
 # ---------------------------------------------------------------------------
@@ -826,12 +948,12 @@ def main():
             ts.append(a0.elapsed_time(a1))
         per_task_ms[task] = round(statistics.median(ts), 4)
 
-    result = {"metric": "GFLOP/s (2×intermediate products/s) A·A & A·Aᵀ",
+    result = {"metric": METRIC,
               "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world,
               "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
               "data": "synthetic (seeded generator)",
-              "config": config(args, A, {"aat_task": args.aat_task}),
+              "config": config(args, A), "aat_task": args.aat_task,
               "roofline": roofline,
               "call_roofline": {"alg_bytes_per_step": int(call_alg),
                                 "achieved": round(call_alg / (ms * 1e-3) / 1e9, 1),
@@ -915,6 +1037,11 @@ def main():
         if all("ms_mean" in cs.get(t, {}) for t in ("AA", "AAt")):
             cms = cs["AA"]["ms_mean"] + cs["AAt"]["ms_mean"]
             result["baselines"]["cusparse_step_gflops"] = round(work_per_step / (cms * 1e-3) / 1e9, 3)
+    if rank == 0 and world == 1 and not args.no_sub:
+        del dA
+        torch.cuda.empty_cache()
+        result["sub_results"] = {"laplace2d_64": laplace_subresult(eng),
+                                 "batch_512": batch_subresult(eng)}
 
     eng.close()
     if world > 1:

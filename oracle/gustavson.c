@@ -324,6 +324,75 @@ int oracle_rows_fill(int32_t n, const int32_t* Ap, const int32_t* Ai, const doub
   return failed ? -1 : 0;
 }
 
+/*
+ * The 27-point stencil on a side³ grid as the benchmark defines it, for the
+ * CPU legs that must not load the engine library: rows in z, y, x order,
+ * neighbours in dz, dy, dx order (each −1..1, inside the grid), so columns
+ * ascend; values um11(x) = 2·((x >> 11)·2^-53) − 1 of consecutive draws x of
+ * MT19937-64 (Matsumoto and Nishimura's 64-bit Mersenne Twister, the engine of
+ * C++'s std::mt19937_64) seeded with `seed`, one draw per entry in CSR order.
+ * rowptr has side³+1 entries; col and val (3·side − 2)³.
+ */
+typedef struct {
+  uint64_t mt[312];
+  int i;
+} mt64_t;
+
+static void mt64_seed(mt64_t* g, uint64_t seed) {
+  g->mt[0] = seed;
+  for (int i = 1; i < 312; ++i)
+    g->mt[i] = 6364136223846793005ULL * (g->mt[i - 1] ^ (g->mt[i - 1] >> 62)) + (uint64_t)i;
+  g->i = 312;
+}
+
+static uint64_t mt64_next(mt64_t* g) {
+  const uint64_t upper = 0xFFFFFFFF80000000ULL, lower = 0x7FFFFFFFULL;
+  const uint64_t mat = 0xB5026F5AA96619E9ULL;
+  if (g->i >= 312) {
+    for (int k = 0; k < 312; ++k) {
+      uint64_t y = (g->mt[k] & upper) | (g->mt[(k + 1) % 312] & lower);
+      g->mt[k] = g->mt[(k + 156) % 312] ^ (y >> 1) ^ ((y & 1ULL) ? mat : 0ULL);
+    }
+    g->i = 0;
+  }
+  uint64_t x = g->mt[g->i++];
+  x ^= (x >> 29) & 0x5555555555555555ULL;
+  x ^= (x << 17) & 0x71D67FFFEDA60000ULL;
+  x ^= (x << 37) & 0xFFF7EEE000000000ULL;
+  x ^= x >> 43;
+  return x;
+}
+
+int64_t oracle_gen_stencil27(int32_t side, uint64_t seed, int32_t* rowptr, int32_t* col,
+                             double* val) {
+  const int64_t s = side;
+  mt64_t g;
+  mt64_seed(&g, seed);
+  int64_t p = 0, row = 0;
+  rowptr[0] = 0;
+  for (int64_t z = 0; z < s; ++z)
+    for (int64_t y = 0; y < s; ++y)
+      for (int64_t x = 0; x < s; ++x) {
+        for (int dz = -1; dz <= 1; ++dz) {
+          const int64_t zz = z + dz;
+          if (zz < 0 || zz >= s) continue;
+          for (int dy = -1; dy <= 1; ++dy) {
+            const int64_t yy = y + dy;
+            if (yy < 0 || yy >= s) continue;
+            for (int dx = -1; dx <= 1; ++dx) {
+              const int64_t xx = x + dx;
+              if (xx < 0 || xx >= s) continue;
+              col[p] = (int32_t)((zz * s + yy) * s + xx);
+              val[p] = 2.0 * ((double)(mt64_next(&g) >> 11) * 0x1.0p-53) - 1.0;
+              ++p;
+            }
+          }
+        }
+        rowptr[++row] = (int32_t)p;
+      }
+  return p;
+}
+
 int oracle_max_threads(void) {
 #ifdef _OPENMP
   return omp_get_max_threads();

@@ -48,6 +48,8 @@ def _load():
         L.oracle_rows_fill.restype = ctypes.c_int
         L.oracle_rows_fill.argtypes = [ctypes.c_int32, _i32p, _i32p, _f64p, _i32p, _i32p, _f64p,
                                        _i32p, ctypes.c_int32, _i64p, _i32p, _f64p, ctypes.c_int]
+        L.oracle_gen_stencil27.restype = ctypes.c_int64
+        L.oracle_gen_stencil27.argtypes = [ctypes.c_int32, ctypes.c_uint64, _i32p, _i32p, _f64p]
         L.oracle_max_threads.restype = ctypes.c_int
         L.oracle_max_threads.argtypes = []
         _lib = L
@@ -69,6 +71,10 @@ def _p(a, t):
 class _Csr:
     def __init__(self, n, rowptr, col, val):
         self.n, self.rowptr, self.col, self.val = n, rowptr, col, val
+
+    @property
+    def nnz(self) -> int:
+        return int(len(self.col))
 
 
 def transpose(A):
@@ -159,6 +165,20 @@ def multiply_rows(A, rows, task: str = "AA", B=None, nthreads: int = 0):
     if rc != 0:
         raise RuntimeError("oracle rows fill failed")
     return cp, ci[:tot], cx[:tot]
+
+
+def gen_stencil27(side: int, seed: int):
+    """The benchmark's 27-point stencil on side³ (gustavson.c: oracle_gen_stencil27),
+    built without the engine library: an object with n, rowptr, col, val."""
+    n = side ** 3
+    nnz = (3 * side - 2) ** 3
+    rp = np.zeros(n + 1, dtype=np.int32)
+    col = np.zeros(nnz, dtype=np.int32)
+    val = np.zeros(nnz, dtype=np.float64)
+    got = _load().oracle_gen_stencil27(side, seed, _p(rp, _i32p), _p(col, _i32p), _p(val, _f64p))
+    if got != nnz:
+        raise RuntimeError(f"stencil generator wrote {got} entries, expected {nnz}")
+    return _Csr(n, rp, col, val)
 
 
 def max_threads() -> int:

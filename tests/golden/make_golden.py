@@ -1,9 +1,9 @@
 """Generate the golden fixtures from the reference's own Python code.
 
-Run in a container where the reference tree is mounted (read-only) at
-REFERENCE_ROOT (default /root/reference):
+Run in a container where the reference tree is mounted (read-only), giving its
+root in the required variable REFERENCE_ROOT:
 
-    python tests/golden/make_golden.py
+    REFERENCE_ROOT=<reference tree> python tests/golden/make_golden.py
 
 For a set of small matrices built by this project's generators it records,
 using the reference's functions unmodified:
@@ -28,7 +28,9 @@ import scipy.sparse as sp
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("REFERENCE_ROOT", "/root/reference")
+REF = os.environ.get("REFERENCE_ROOT")
+if not REF or not os.path.isdir(REF):
+    sys.exit("make_golden.py: set REFERENCE_ROOT to the reference tree's root")
 sys.path.insert(0, REPO)
 
 from appt_spgemm_b200 import csr  # noqa: E402

@@ -41,6 +41,28 @@ def test_reference_arm_prints_the_contract_line():
     assert e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
 
 
+def test_reference_arm_loads_no_engine_code_and_keeps_the_config():
+    """The reference arm maps only the oracle's library (never the engine's),
+    and its config is the one the GPU arm prints for the same workload."""
+    import types
+
+    import bench
+    code = ("import runpy, sys; sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', "
+            "'--warmup', '3']; runpy.run_path('bench.py', run_name='__main__'); "
+            "print(open('/proc/self/maps').read(), file=sys.stderr)")
+    p = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True,
+                       timeout=600)
+    assert p.returncode == 0, p.stderr[-2000:]
+    assert "liboracle.so" in p.stderr
+    assert "libspgemm_b200" not in p.stderr
+    d = json.loads(p.stdout.strip().splitlines()[-1])
+    side = 96
+    A = types.SimpleNamespace(n=side ** 3, nnz=(3 * side - 2) ** 3)
+    args = types.SimpleNamespace(side=side, gpus=1)
+    assert d["config"] == json.loads(json.dumps(bench.config(args, A)))
+    assert "every row" in d["cpu_baseline"]["sample"]
+
+
 def test_reference_arm_other_ranks_print_nothing():
     p = run_bench({"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"})
     assert p.returncode == 0, p.stderr[-2000:]

@@ -313,23 +313,63 @@ def test_cli_protocol(golden_dir):
 
 
 def test_stencil27_full_size_properties(eng):
-    """The 27-point stencil on 96³ at full size: A·A bit-exact against the
-    oracle, nnz(C) equal to the 5×5×5-stencil count, and the Gram path
-    bit-identical to the plain A·Aᵀ."""
+    """The 27-point stencil on 96³ at full size, both products of the benchmark
+    step: A·A and A·Aᵀ bit-exact against the oracle, nnz(C) equal to the
+    5×5×5-stencil count, and the Gram path bit-identical to the plain A·Aᵀ."""
     A = csr.stencil27(96, seed=2)
     d = dev(A)
-    C = eng.multiply(d, "AA")
-    torch.cuda.synchronize()
     s = np.array([3, 4] + [5] * 92 + [4, 3], dtype=np.int64)  # reachable offsets per axis
-    assert C.nnz == int(s.sum() ** 3) == 106496000 or C.nnz == int((s.sum()) ** 3)
-    assert_same(C, oracle.multiply(A, "AA", nthreads=0), "stencil27_96/AA")
-    del C
+    want_nnz = int(s.sum()) ** 3
+    assert want_nnz == 106496424
+    for task in ("AA", "AAt"):
+        C = eng.multiply(d, task)
+        torch.cuda.synchronize()
+        assert C.nnz == want_nnz, task
+        assert_same(C, oracle.multiply(A, task, nthreads=0), f"stencil27_96/{task}")
+        del C
     G = eng.multiply(d, "AAtS")
     P = eng.multiply(d, "AAt")
     torch.cuda.synchronize()
-    assert G.nnz == P.nnz
+    assert G.nnz == P.nnz == want_nnz
     assert torch.equal(G.rowptr, P.rowptr) and torch.equal(G.col, P.col)
     assert torch.equal(G.val.view(torch.int64), P.val.view(torch.int64))
+
+
+REF_ENGINE = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                          "oracle", "_ref", "spgemm_ref")
+
+
+def rel_ok(a, b, rt=1e-6):
+    """The reference sweep's checksum tolerance (bench/run_compare.py:42-43)."""
+    return abs(a - b) <= rt * max(1.0, abs(b))
+
+
+@pytest.mark.parametrize("name", ["laplace2d_64", "stencil27_96"])
+def test_against_reference_engine(eng, name, tmp_path):
+    """The benchmark matrices through the reference's own CUDA engine
+    (src/spgemm.cu, built unmodified into oracle/_ref/): nnz(C) equal and the
+    three checksums within the reference's own tolerance, for every task,
+    with the engine's C checksummed like the reference's run_ours does
+    (src/spgemm_engine.cuh:116-118)."""
+    if not os.path.exists(REF_ENGINE):
+        pytest.skip("the reference engine was not built (oracle/Makefile REF=...)")
+    A = csr.laplace2d(64) if name == "laplace2d_64" else csr.stencil27(96, seed=2)
+    path = str(tmp_path / "a.csr")
+    csr.write_bin(A, path)
+    d = dev(A)
+    for task in TASKS:
+        out = subprocess.run([REF_ENGINE, name, path, task, "1"], capture_output=True, text=True,
+                             timeout=600, check=True).stdout
+        chk = re.findall(r"__chk s=(\S+) as=(\S+) sq=(\S+)", out)
+        res = [ln.split(",") for ln in out.splitlines() if ln.startswith("RESULT,")]
+        assert len(chk) == 1 and len(res) == 1, out
+        C = eng.multiply(d, task)
+        torch.cuda.synchronize()
+        assert C.nnz == int(res[0][5]), f"{name}/{task}: nnz {C.nnz} vs {res[0][5]}"
+        ours = oracle.checksum(C.val.cpu().numpy())
+        for got, want in zip(ours, (float(x) for x in chk[0])):
+            assert rel_ok(got, want), f"{name}/{task}: checksum {got} vs reference {want}"
+        del C
 
 
 def prune(ref):
