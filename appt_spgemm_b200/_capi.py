@@ -67,7 +67,8 @@ class SpgPlanInfo(Structure):
                 ("products", c_int64), ("products_computed", c_int64),
                 ("max_row_products", c_int64), ("max_row_nnz", c_int64),
                 ("heavy_rows", c_int64), ("workspace_bytes", c_int64),
-                ("output_bytes", c_int64), ("bins_used", c_int32), ("symmetric_pattern", c_int32)]
+                ("output_bytes", c_int64), ("bins_used", c_int32), ("symmetric_pattern", c_int32),
+                ("exec_workspace_bytes", c_int64)]
 
 
 class SpgDescriptors(Structure):
@@ -91,7 +92,7 @@ class SpgRequestInfo(Structure):
     _fields_ = [("id", c_uint64), ("status", c_int32), ("task", c_int32), ("n", c_int32),
                 ("batched", c_int32), ("nnz_c", c_int64), ("products", c_int64),
                 ("reserved_bytes", c_int64), ("submit_ms", c_double), ("start_ms", c_double),
-                ("done_ms", c_double)]
+                ("done_ms", c_double), ("planned_ms", c_double), ("run_ms", c_double)]
 
 
 class SpgServerStats(Structure):
@@ -99,7 +100,8 @@ class SpgServerStats(Structure):
                 ("failed", c_int64), ("batches", c_int64), ("products_completed", c_int64),
                 ("budget_bytes", c_int64), ("reserved_bytes", c_int64),
                 ("peak_reserved_bytes", c_int64), ("p50_ms", c_double), ("p99_ms", c_double),
-                ("max_ms", c_double), ("first_submit_ms", c_double), ("last_done_ms", c_double)]
+                ("max_ms", c_double), ("first_submit_ms", c_double), ("last_done_ms", c_double),
+                ("held_bytes", c_int64), ("peak_held_bytes", c_int64)]
 
 
 _ctx_p = c_void_p
@@ -117,6 +119,8 @@ SIGNATURES = {
     "spg_plan_create": (c_int32, [_ctx_p, c_int32, POINTER(SpgCsrDev), c_void_p,
                                   POINTER(_plan_p)]),
     "spg_plan_get_info": (c_int32, [_plan_p, POINTER(SpgPlanInfo)]),
+    "spg_plan_workspace_bound": (c_int32, [_ctx_p, c_int32, c_int32, POINTER(SpgCsrDev), c_int32,
+                                           POINTER(c_int64)]),
     "spg_execute": (c_int32, [_plan_p, POINTER(SpgCsrOut), c_void_p]),
     "spg_plan_destroy": (c_int32, [_plan_p]),
     "spg_multiply": (c_int32, [_ctx_p, c_int32, POINTER(SpgCsrDev), POINTER(SpgCsrOut),

@@ -143,7 +143,7 @@ struct spg_plan {
   int64_t* blk_off = nullptr;
   uint16_t* blk_cnt = nullptr;
   int blk_log2 = 12;
-  int4* hcur = nullptr;
+  bool heavy_windows = false;  // the windowed heavy kernel runs: execute takes its cursors
   int32_t* hqueue = nullptr;  // next row of the CTA-per-row kernels (zeroed before each launch)
   int window_bits = 1 << 20;  // heavy-path shape (heavy_shape)
   int heavy_threads = 1024;
@@ -321,6 +321,44 @@ spg_status validate_device(spg_ctx* ctx, const MatView& A, cudaStream_t st,
   const uint32_t* h = (const uint32_t*)ctx->h_pin;
   if (symmetric) *symmetric = h[1] == 0;
   return status_from_bits(h[0]);
+}
+
+// Bytes execute_impl takes from the pool for the duration of an execute for
+// the Gram mirror: its cursors, lower parts and segment-sort list (0 for the
+// other tasks; the heavy rows' cursors are added by the caller).
+int64_t exec_workspace(int64_t n, bool gram, int64_t nnz_low) {
+  if (!gram) return 0;
+  const int64_t nn = n > 0 ? n : 1;
+  return 4 * nn + 12 * (nnz_low > 0 ? nnz_low : 1) + 4 * nn + 4;
+}
+
+// Upper bound of the workspace plan_build allocates (a plan's workspace_bytes)
+// for a matrix of n rows and nnz entries, from the sizes alone: every palloc of
+// plan_build at its largest (the transpose counted whenever the task needs
+// Aᵀ, the heavy-row counts and cursors always).  The serving loop reserves it
+// against its budget before planning.
+int64_t plan_workspace_bound(const spg_config& cfg, spg_task task, int64_t n, int64_t nnz) {
+  const int64_t nn = n > 0 ? n : 1, nz = nnz > 0 ? nnz : 1;
+  const int64_t scan = (int64_t)scan_tmp_bytes(n);
+  const int64_t nblocks = (n + kBinRowsPerBlock - 1) / kBinRowsPerBlock;
+  int64_t b = 0;
+  if (task != SPG_TASK_AA) {
+    b += 8 * nz;                                  // values of Aᵀ
+    b += 4 * (nn + 1) + 4 * nz + 4 * nn + 4 * nn  // Aᵀ rowptr/col, counts, cursors
+         + scan + 4 * nz + 8 * nz + 4 * nn + 4;   // scan, staging copy, long list
+  }
+  b += 8 * nn + 4 * nn + 4 * nn + 4;                              // f, lo, hi, queue
+  b += 4 * kNumBins * (nblocks > 0 ? nblocks : 1) + 8 * 4 * kNumBins + 4 * nn;  // binning
+  b += 4 * nn + 8 * (nn + 1) + scan;                              // heavy block offsets
+  const int64_t per_row_blocks = (nn + 1023) / 1024 + 1;
+  const int64_t blocks = nn > cfg.heavy_block_budget / per_row_blocks ? cfg.heavy_block_budget
+                                                                      : nn * per_row_blocks;
+  b += 2 * blocks;                                                // heavy block counts
+  b += 4 * nn;                                                    // row counts
+  if (task == SPG_TASK_AATS) b += 4 * nn + scan + 8 * (nn + 1);   // lower counts, offsets
+  b += scan + 8 * (nn + 1);                                       // C row pointers
+  b += 4 * nn + 32;                                               // numeric rows, stats
+  return b + 64 * 1024;  // pool rounding of the ~40 allocations
 }
 
 void plan_free(spg_plan* p) {
@@ -561,12 +599,14 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
   p->info.max_row_products = (int64_t)sv[1];
   p->info.max_row_nnz = (int64_t)sv[2];
   p->info.heavy_rows = p->num_count[kHeavyBin];
-  if (p->num_count[kHeavyBin] > 0 && p->blk_cnt) TRY(palloc(p, &p->hcur, Ad->nnz));
+  p->heavy_windows = p->num_count[kHeavyBin] > 0 && p->blk_cnt;
   for (int b = 1; b < kNumBins; ++b)
     if (p->num_count[b] > 0) ++bins_used;
   p->info.bins_used = bins_used;
   p->info.output_bytes = 8 * ((int64_t)n + 1) + 12 * p->nnz_c;
   p->info.workspace_bytes = p->ws_bytes;
+  p->info.exec_workspace_bytes = exec_workspace(n, gram, p->nnz_low) +
+                                 (p->heavy_windows ? 16 * Ad->nnz : 0);
   return SPG_OK;
 }
 
@@ -664,12 +704,16 @@ spg_status execute_impl(spg_plan* p, spg_csr_out* C, cudaStream_t st) {
       h.cap = heavy_cap(ctx->cfg.num_load_pct);
       h.sub_log2 = 31 - __builtin_clz((unsigned)h.cap);  // largest power of two <= cap
       if (h.sub_log2 > p->blk_log2) h.sub_log2 = p->blk_log2;
-      h.hcur = p->hcur;
+      if (p->heavy_windows) {  // one int4 cursor per entry of A
+        void* hc;
+        if ((result = talloc(&hc, sizeof(int4) * (size_t)p->A.nnz)) != SPG_OK) break;
+        h.hcur = (int4*)hc;
+      }
       h.queue = p->hqueue;
       // rows fed by many short B rows stream through the warp kernel's
       // windows; rows dominated by long B rows, rows of more than 2^17
       // products, or all rows without block counts take the CTA kernel
-      const bool windows = p->blk_cnt && p->hcur;
+      const bool windows = p->heavy_windows;
       h.f = p->f;
       h.split = !windows ? 0
                 : ctx->cfg.heavy_split > 0 ? (int64_t)ctx->cfg.heavy_split : kHeavySplitDefault;
@@ -935,6 +979,27 @@ spg_status spg_plan_create_batched(spg_ctx* ctx, spg_task task, int32_t count,
     return s;
   }
   *out = p;
+  return SPG_OK;
+}
+
+spg_status spg_plan_workspace_bound(const spg_ctx* ctx, spg_task task, int32_t count,
+                                    const spg_csr_dev* As, int32_t batched, int64_t* bytes) {
+  begin_call();
+  if (!ctx || !As || !bytes || count < 1 || (!batched && count != 1))
+    return set_error(SPG_ERR_INVALID_ARG, "null argument, count < 1, or count != 1 unbatched");
+  if (task != SPG_TASK_AA && task != SPG_TASK_AAT && task != SPG_TASK_AATS)
+    return set_error(SPG_ERR_INVALID_ARG, "unknown task %d", (int)task);
+  int64_t N = 0, NNZ = 0;
+  for (int32_t b = 0; b < count; ++b) {
+    if (As[b].n < 0 || As[b].nnz < 0) return set_error(SPG_ERR_INVALID_ARG, "negative n or nnz");
+    N += As[b].n;
+    NNZ += As[b].nnz;
+  }
+  int64_t w = plan_workspace_bound(ctx->cfg, task, N, NNZ);
+  if (batched)  // the block-diagonal copy, column bases, instance table and offsets
+    w += 4 * (N + 1) + 12 * (NNZ > 0 ? NNZ : 1) + 4 * (N > 0 ? N : 1) +
+         (int64_t)sizeof(BatchDesc) * count + 3 * 8 * ((int64_t)count + 1);
+  *bytes = w;
   return SPG_OK;
 }
 

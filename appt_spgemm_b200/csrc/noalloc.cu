@@ -12,6 +12,9 @@
 // copy of the entries, long-segment list) is g_noalloc_scratch below: about
 // 6.8 MB held by every GPU that loads the library until the process exits.
 // It bounds the input to n <= kNoAllocMaxN rows and nnz <= kNoAllocMaxNnz.
+// The call runs on the current device; A and the outputs must live there.
+// The array's device address is resolved once per device and kept, so the
+// library must not be used across a cudaDeviceReset of that device.
 #include <cstdio>
 #include <mutex>
 
@@ -71,6 +74,19 @@ spg_status scratch_for_current_device(unsigned char** out, int* num_sms) {
   return SPG_OK;
 }
 
+// A device pointer that belongs to another GPU than the current one: the call
+// would run its kernels (and its scratch) on the current device and reach the
+// buffer through peer access.  Host, managed and unregistered pointers pass.
+bool on_other_device(const void* p, int dev) {
+  if (!p) return false;
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeDevice && at.device != dev;
+}
+
 }  // namespace
 
 extern "C" spg_status spg_transpose_noalloc(const spg_csr_dev* A, int32_t* t_rowptr,
@@ -89,6 +105,14 @@ extern "C" spg_status spg_transpose_noalloc(const spg_csr_dev* A, int32_t* t_row
                      (long long)A->nnz);
   if (spg::scan_tmp_bytes(A->n) > kScanBytes)
     return set_error(SPG_ERR_UNSUPPORTED, "scan partials exceed the static scratch");
+  int cur = 0;
+  if (cudaGetDevice(&cur) != cudaSuccess) return set_error(SPG_ERR_CUDA, "no current device");
+  if (on_other_device(A->rowptr, cur) || on_other_device(A->col, cur) ||
+      on_other_device(A->val, cur) || on_other_device(t_rowptr, cur) ||
+      on_other_device(t_col, cur) || on_other_device(t_val, cur))
+    return set_error(SPG_ERR_INVALID_ARG,
+                     "spg_transpose_noalloc runs on the current device (%d); an input or output "
+                     "buffer lives on another GPU", cur);
   unsigned char* s = nullptr;
   int num_sms = 0;
   spg_status st = scratch_for_current_device(&s, &num_sms);

@@ -15,12 +15,17 @@
 //    has the highest priority and the other workers' launches use one CTA per
 //    work item (no persistent grids), so small requests' CTAs interleave with
 //    a large product's instead of waiting for it to finish;
-//  - after planning, a job's exact output size plus the plan workspace is
-//    reserved against the budget.  A job that can never fit is rejected (a
-//    batch is split into its requests first); a job that does not fit yet is
-//    kept, planned, in the worker's waiting list (at most two) while the
-//    worker takes other work, and runs as soon as releases make room, oldest
-//    first.
+//  - admission is by a device-memory budget that covers every byte the
+//    server holds: before planning, a job reserves an upper bound of its plan
+//    workspace (spg_plan_workspace_bound, from the input sizes); after the
+//    symbolic pass it needs its exact outputs plus the workspace of the plan and
+//    of its execute.  A job that can never fit is rejected (a batch is split
+//    into its requests first).  A job that does not fit yet holds nothing: its
+//    plan is destroyed and it waits, with its exact need, in the worker's
+//    waiting list while the worker takes other work; it is planned again and
+//    runs as soon as releases make room, oldest first.  The server also counts
+//    the bytes it actually holds (plans, execute workspace, results) and keeps
+//    their peak, which never exceeds the budget.
 // The reference has no serving layer; this follows the serving contract of
 // the benchmark configuration (Poisson arrivals, p50/p99 latency).
 #include <cuda_runtime.h>
@@ -50,10 +55,11 @@ struct Request {
   int32_t status = SPG_ERR_NOT_READY;
   bool batched = false;
   int64_t nnz_c = 0, products = 0, reserved = 0;
-  double submit_ms = 0, start_ms = 0, done_ms = 0;
+  double submit_ms = 0, start_ms = 0, planned_ms = 0, run_ms = 0, done_ms = 0;
   int64_t* rowptr = nullptr;
   int32_t* col = nullptr;
   double* val = nullptr;
+  int copying = 0;  // spg_server_copy_result calls reading the result right now
   std::string error;
 };
 
@@ -78,6 +84,7 @@ struct spg_server {
   std::unordered_map<uint64_t, std::unique_ptr<Request>> reqs;
   uint64_t next_id = 1;
   int64_t reserved = 0, peak = 0, batches = 0;
+  int64_t held = 0, held_peak = 0;  // bytes of plans, execute workspace and results alive
   bool stopping = false;
   std::vector<std::thread> workers;
 
@@ -119,11 +126,18 @@ struct Job {
   spg_plan_info info{};
   std::vector<int64_t> row_off, nnz_off, out_r;  // merged batches
   int64_t outs = 0;  // result bytes, reserved until the client releases them
-  int64_t temp = 0;  // workspace (and, for a batch, the concatenated C) for the run
+  int64_t temp = 0;  // plan + execute workspace (and, for a batch, the concatenated C)
+  int64_t pre = 0;   // reserved before planning: the workspace bound, or the exact need
+  bool known = false;  // planned before: pre is the exact need
   int64_t need() const { return outs + temp; }
 };
 
-constexpr size_t kMaxWaiting = 2;  // planned jobs a worker keeps while it takes new work
+constexpr size_t kMaxWaiting = 4;  // jobs (holding no memory) a worker keeps waiting
+
+void hold(spg_server* s, int64_t bytes) {  // caller holds the lock
+  s->held += bytes;
+  s->held_peak = std::max(s->held_peak, s->held);
+}
 
 // Queue the requests of batch `j` as single-request jobs.  The worker takes
 // jobs from the back of `split`, so they go in newest first and run in
@@ -150,10 +164,12 @@ bool plan_job(spg_server* s, spg_ctx* ctx, cudaStream_t st, Job& j, std::vector<
     }
     spg_plan_get_info(j.p, &j.info);
     j.outs = output_bytes(r->A.n, j.info.nnz_c);
-    j.temp = j.info.workspace_bytes;
+    j.temp = j.info.workspace_bytes + j.info.exec_workspace_bytes;
     std::lock_guard<std::mutex> lk(s->mu);
+    hold(s, j.info.workspace_bytes);
     r->products = j.info.products;
     r->nnz_c = j.info.nnz_c;
+    r->planned_ms = s->now_ms();
     return true;
   }
   std::vector<spg_csr_dev> As;
@@ -174,17 +190,35 @@ bool plan_job(spg_server* s, spg_ctx* ctx, cudaStream_t st, Job& j, std::vector<
     j.out_r[i] = output_bytes(j.rs[i]->A.n, j.nnz_off[i + 1] - j.nnz_off[i]);
     j.outs += j.out_r[i];
   }
-  j.temp = output_bytes(j.info.n, j.info.nnz_c) + j.info.workspace_bytes;
+  j.temp = output_bytes(j.info.n, j.info.nnz_c) + j.info.workspace_bytes +
+           j.info.exec_workspace_bytes;
+  std::lock_guard<std::mutex> lk(s->mu);
+  hold(s, j.info.workspace_bytes);
+  const double t = s->now_ms();
+  for (Request* r : j.rs) r->planned_ms = t;
   return true;
+}
+
+// Destroy a job's plan and stop counting its workspace.
+void drop_plan(spg_server* s, Job& j) {
+  if (!j.p) return;
+  spg_plan_destroy(j.p);
+  j.p = nullptr;
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->held -= j.info.workspace_bytes;
 }
 
 // Execute an admitted job (its need is reserved) and finish its requests.
 void run_job(spg_server* s, cudaStream_t st, Job& j) {
   spg_status rc = SPG_OK;
   const bool batch = j.rs.size() > 1;
+  const int64_t run_extra = j.temp - j.info.workspace_bytes;  // execute workspace (+ batch C)
   {
     std::lock_guard<std::mutex> lk(s->mu);
     if (batch) ++s->batches;
+    hold(s, run_extra + j.outs);
+    const double t = s->now_ms();
+    for (Request* r : j.rs) r->run_ms = t;
     for (size_t b = 0; b < j.rs.size(); ++b) {
       Request* r = j.rs[b];
       r->batched = batch;
@@ -221,12 +255,12 @@ void run_job(spg_server* s, cudaStream_t st, Job& j) {
   }
   if (rc == SPG_OK && cudaStreamSynchronize(st) != cudaSuccess) rc = SPG_ERR_CUDA;
   const std::string err = rc == SPG_OK ? "" : spg_last_error_string();
-  spg_plan_destroy(j.p);
-  j.p = nullptr;
+  drop_plan(s, j);
   if (rc != SPG_OK)
     for (Request* r : j.rs) free_result(r, st);
   {
     std::lock_guard<std::mutex> lk(s->mu);
+    s->held -= run_extra + (rc == SPG_OK ? 0 : j.outs);
     s->reserved -= j.temp + (rc == SPG_OK ? 0 : j.outs);
     for (size_t b = 0; b < j.rs.size(); ++b) {
       Request* r = j.rs[b];
@@ -268,13 +302,38 @@ bool take_requests(spg_server* s, bool small_only, std::vector<Request*>& rs) {
   return true;
 }
 
-// Admission after planning: reject what can never fit, reserve what fits now,
-// otherwise keep it waiting (with its plan) while the worker takes other work.
+// Admission before planning: reserve `pre` (the workspace bound of a new job,
+// or the exact need of one planned before).  A job whose `pre` exceeds the
+// whole budget can never run: a batch is split into its requests, a single
+// request is rejected.
 enum class Admit { kRun, kWait, kRejected };
-Admit admit(spg_server* s, Job& j, std::vector<Job>& split) {
+Admit admit_pre(spg_server* s, Job& j, std::vector<Job>& split) {
   std::lock_guard<std::mutex> lk(s->mu);
+  if (j.pre > s->cfg.memory_budget_bytes) {
+    if (j.rs.size() > 1) {
+      split_into_requests(j, split);
+    } else {
+      finish(s, j.rs[0], SPG_ERR_BUDGET, "request exceeds the memory budget");
+    }
+    return Admit::kRejected;
+  }
+  if (s->reserved + j.pre <= s->cfg.memory_budget_bytes) {
+    s->reserved += j.pre;
+    s->peak = std::max(s->peak, s->reserved);
+    return Admit::kRun;
+  }
+  return Admit::kWait;
+}
+
+// Admission after planning (its `pre` is reserved): trade it for the exact
+// need.  kRun: the need is reserved.  kWait: the need does not fit now; `pre`
+// is returned and becomes the need (the caller drops the plan and keeps the
+// job waiting).  kRejected: the need exceeds the whole budget.
+Admit admit_planned(spg_server* s, Job& j, std::vector<Job>& split) {
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->reserved -= j.pre;
   if (j.need() > s->cfg.memory_budget_bytes) {
-    if (j.rs.size() > 1) {  // a batch too large for the budget: try its requests one by one
+    if (j.rs.size() > 1) {
       split_into_requests(j, split);
     } else {
       finish(s, j.rs[0], SPG_ERR_BUDGET, "request exceeds the memory budget");
@@ -286,6 +345,8 @@ Admit admit(spg_server* s, Job& j, std::vector<Job>& split) {
     s->peak = std::max(s->peak, s->reserved);
     return Admit::kRun;
   }
+  j.pre = j.need();
+  j.known = true;
   return Admit::kWait;
 }
 
@@ -307,68 +368,90 @@ void worker_main(spg_server* s, int index) {
   if (s->cfg.workers >= 2 && !small_only) cfg.grid_sms = 1 << 16;
   spg_ctx* ctx = nullptr;
   const bool ok = spg_create(&ctx, &cfg) == SPG_OK;
-  std::deque<Job> waiting;  // planned, not admitted yet, oldest first
-  std::vector<Job> todo;    // taken or split off, to be planned
+  std::deque<Job> waiting;  // admitted to nothing, holding no memory, oldest first
+  std::vector<Job> todo;    // taken or split off, to be admitted and planned
   for (;;) {
     Job job;
-    bool run_now = false;
+    bool reserved = false;  // job.pre is reserved
     if (todo.empty()) {
       std::unique_lock<std::mutex> lk(s->mu);
+      bool have = false;
       for (;;) {
         if (!waiting.empty() &&
-            s->reserved + waiting.front().need() <= s->cfg.memory_budget_bytes) {
+            s->reserved + waiting.front().pre <= s->cfg.memory_budget_bytes) {
           job = std::move(waiting.front());
           waiting.pop_front();
-          s->reserved += job.need();
+          s->reserved += job.pre;
           s->peak = std::max(s->peak, s->reserved);
-          run_now = true;
+          reserved = have = true;
           break;
         }
         std::vector<Request*> rs;
         if (waiting.size() < kMaxWaiting && take_requests(s, small_only, rs)) {
-          Job j;
-          j.rs = std::move(rs);
-          todo.push_back(std::move(j));
+          job.rs = std::move(rs);
+          have = true;
           break;
         }
         if (s->stopping) break;
         s->cv_work.wait(lk);
       }
-      if (!run_now && todo.empty()) {  // stopping: what still waits does not run
+      if (!have) {  // stopping: what still waits does not run
         for (Job& j : waiting)
           for (Request* r : j.rs) finish(s, r, SPG_ERR_CUDA, "server stopped before the request ran");
-        lk.unlock();
-        for (Job& j : waiting) spg_plan_destroy(j.p);
         waiting.clear();
+        lk.unlock();
         s->cv_done.notify_all();
         break;
       }
+    } else {
+      job = std::move(todo.back());
+      todo.pop_back();
     }
-    if (run_now) {
-      run_job(s, st, job);
-      continue;
-    }
-    job = std::move(todo.back());
-    todo.pop_back();
     if (!ok) {
       std::lock_guard<std::mutex> lk(s->mu);
+      if (reserved) s->reserved -= job.pre;
       for (Request* r : job.rs) finish(s, r, SPG_ERR_CUDA, "worker context could not be created");
       s->cv_done.notify_all();
       continue;
     }
-    if (!plan_job(s, ctx, st, job, todo)) {
+    if (!reserved) {
+      std::vector<spg_csr_dev> As;
+      for (Request* r : job.rs) As.push_back(r->A);
+      if (spg_plan_workspace_bound(ctx, job.rs[0]->task, (int32_t)As.size(), As.data(),
+                                   As.size() > 1 ? 1 : 0, &job.pre) != SPG_OK)
+        job.pre = 0;
+      const Admit a = admit_pre(s, job, todo);
+      if (a == Admit::kRejected) {
+        s->cv_done.notify_all();
+        continue;
+      }
+      if (a == Admit::kWait) {
+        waiting.push_back(std::move(job));
+        continue;
+      }
+    }
+    const int64_t pre = job.pre;
+    if (!plan_job(s, ctx, st, job, todo)) {  // failed: finished or split
+      {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->reserved -= pre;
+      }
+      s->cv_work.notify_all();
       s->cv_done.notify_all();
       continue;
     }
-    switch (admit(s, job, todo)) {
+    switch (admit_planned(s, job, todo)) {
       case Admit::kRun:
         run_job(s, st, job);
         break;
       case Admit::kWait:
+        drop_plan(s, job);
         waiting.push_back(std::move(job));
+        s->cv_work.notify_all();  // its workspace reservation was returned
         break;
       case Admit::kRejected:
-        spg_plan_destroy(job.p);
+        drop_plan(s, job);
+        s->cv_work.notify_all();
         s->cv_done.notify_all();
         break;
     }
@@ -441,6 +524,8 @@ static void fill_info(const Request* r, spg_request_info* info) {
   info->submit_ms = r->submit_ms;
   info->start_ms = r->start_ms;
   info->done_ms = r->done_ms;
+  info->planned_ms = r->planned_ms;
+  info->run_ms = r->run_ms;
 }
 
 spg_status spg_server_poll(spg_server* s, uint64_t id, spg_request_info* info) {
@@ -488,13 +573,20 @@ spg_status spg_server_copy_result(spg_server* s, uint64_t id, int64_t* rowptr, i
     if (r->status != SPG_OK || !r->rowptr)
       return spg::set_error(SPG_ERR_NOT_READY, "request %llu has no result (status %d)",
                             (unsigned long long)id, r->status);
+    if (r->nnz_c > 0 && (!col || !val)) return spg::set_error(SPG_ERR_INVALID_ARG, "null col/val");
+    // pin the result: spg_server_release waits until no copy reads it
+    ++r->copying;
   }
   cudaError_t e = cudaMemcpy(rowptr, r->rowptr, 8 * ((size_t)r->A.n + 1), cudaMemcpyDefault);
   if (e == cudaSuccess && r->nnz_c > 0) {
-    if (!col || !val) return spg::set_error(SPG_ERR_INVALID_ARG, "null col/val");
     e = cudaMemcpy(col, r->col, 4 * (size_t)r->nnz_c, cudaMemcpyDefault);
     if (e == cudaSuccess) e = cudaMemcpy(val, r->val, 8 * (size_t)r->nnz_c, cudaMemcpyDefault);
   }
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    --r->copying;
+  }
+  s->cv_done.notify_all();
   if (e != cudaSuccess) return spg::set_error(SPG_ERR_CUDA, "copy: %s", cudaGetErrorString(e));
   return SPG_OK;
 }
@@ -504,17 +596,20 @@ spg_status spg_server_release(spg_server* s, uint64_t id) {
   if (!s) return spg::set_error(SPG_ERR_INVALID_ARG, "null server");
   int64_t bytes = 0;
   {
-    std::lock_guard<std::mutex> lk(s->mu);
+    std::unique_lock<std::mutex> lk(s->mu);
     auto it = s->reqs.find(id);
     if (it == s->reqs.end())
       return spg::set_error(SPG_ERR_INVALID_ARG, "unknown request %llu", (unsigned long long)id);
     Request* r = it->second.get();
     if (r->status == SPG_ERR_NOT_READY)
       return spg::set_error(SPG_ERR_NOT_READY, "request %llu still running", (unsigned long long)id);
+    // copies of this result started by other threads finish first
+    s->cv_done.wait(lk, [&] { return r->copying == 0; });
     free_result(r, nullptr);
     bytes = r->reserved;
     r->reserved = 0;
     s->reserved -= bytes;
+    s->held -= bytes;
   }
   s->cv_work.notify_all();
   return SPG_OK;
@@ -555,6 +650,8 @@ spg_status spg_server_stats_get(spg_server* s, spg_server_stats* st) {
   st->budget_bytes = s->cfg.memory_budget_bytes;
   st->reserved_bytes = s->reserved;
   st->peak_reserved_bytes = s->peak;
+  st->held_bytes = s->held;
+  st->peak_held_bytes = s->held_peak;
   return SPG_OK;
 }
 

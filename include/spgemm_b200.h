@@ -145,6 +145,7 @@ typedef struct spg_plan_info {
   int64_t output_bytes;       /* 8(n+1) + 12·nnz_c                              */
   int32_t bins_used;
   int32_t symmetric_pattern;  /* A·Aᵀ tasks: 1 when Aᵀ reused A's pattern      */
+  int64_t exec_workspace_bytes; /* taken from the pool during each execute      */
 } spg_plan_info;
 
 /* Structural descriptors of A (the reference's dispatcher features,
@@ -188,6 +189,14 @@ spg_status spg_check_device_status(spg_ctx* ctx, void* stream);
 spg_status spg_plan_create(spg_ctx* ctx, spg_task task, const spg_csr_dev* A,
                            void* stream, spg_plan** plan);
 spg_status spg_plan_get_info(const spg_plan* plan, spg_plan_info* info);
+/* Upper bound of the plan workspace (spg_plan_info.workspace_bytes) that
+ * spg_plan_create (batched = 0, count = 1) or spg_plan_create_batched
+ * (batched = 1) would allocate for these inputs under ctx's configuration,
+ * from their sizes alone (no device work): what a caller with a memory budget
+ * reserves before planning.  The reference has no counterpart (its run_ours
+ * allocates per call, src/spgemm_engine.cuh:137-181). */
+spg_status spg_plan_workspace_bound(const spg_ctx* ctx, spg_task task, int32_t count,
+                                    const spg_csr_dev* As, int32_t batched, int64_t* bytes);
 /* Numeric phase + in-row sort (+ mirror for AAtS) into caller-owned buffers:
  * C->rowptr (n+1), C->col / C->val (info.nnz_c).  Asynchronous on `stream`.
  * A plan fixes the structure only: a plan may be executed again after A's
@@ -260,8 +269,10 @@ typedef struct spg_request_info {
                                   the request's share of the output            */
   int64_t reserved_bytes;
   double submit_ms;            /* host clock, ms since the server started       */
-  double start_ms;
+  double start_ms;             /* a worker took it from the queue               */
   double done_ms;              /* the GPU finished this request's product        */
+  double planned_ms;           /* its (last) symbolic pass ended                */
+  double run_ms;               /* admitted with its exact need; execute began   */
 } spg_request_info;
 
 typedef struct spg_server_stats {
@@ -270,6 +281,9 @@ typedef struct spg_server_stats {
   int64_t budget_bytes, reserved_bytes, peak_reserved_bytes;
   double p50_ms, p99_ms, max_ms;   /* latency submit → done of completed requests */
   double first_submit_ms, last_done_ms;
+  int64_t held_bytes;          /* device bytes the server holds now: plans,
+                                  execute workspace, results not yet released */
+  int64_t peak_held_bytes;     /* their peak; never above budget_bytes          */
 } spg_server_stats;
 
 spg_status spg_server_create(const spg_server_config* cfg, spg_server** out);
@@ -280,10 +294,13 @@ spg_status spg_server_poll(spg_server* s, uint64_t id, spg_request_info* info);
  * timeout_ms (negative: no limit). */
 spg_status spg_server_wait(spg_server* s, uint64_t id, int32_t timeout_ms, spg_request_info* info);
 /* Copy a finished result into caller buffers (device or host): rowptr n+1
- * int64, col/val nnz_c.  The server keeps the result until released. */
+ * int64, col/val nnz_c (col and val are checked before anything is copied).
+ * The server keeps the result until released; a release issued by another
+ * thread during the copy waits for the copy to end. */
 spg_status spg_server_copy_result(spg_server* s, uint64_t id, int64_t* rowptr, int32_t* col,
                                   double* val);
-/* Drop a finished result: frees its device memory and returns its budget. */
+/* Drop a finished result: frees its device memory and returns its budget,
+ * after any copy of it still running in another thread has ended. */
 spg_status spg_server_release(spg_server* s, uint64_t id);
 spg_status spg_server_stats_get(spg_server* s, spg_server_stats* st);
 /* Stops the workers: requests running on the device finish; a request that
@@ -333,10 +350,15 @@ spg_status spg_transpose(spg_ctx* ctx, const spg_csr_dev* A, int32_t* t_rowptr,
  * (rowptr n+1, col/val nnz), no context.  Its scratch is a static device array
  * of about 6.8 MB that every GPU loading the library holds until exit, which
  * limits A to n <= 65,536 and nnz <= 524,288 (larger inputs: SPG_ERR_UNSUPPORTED).
- * The first call on each device resolves that array's address (set-up); make
- * it before any stream capture.  All calls share the array: calls that
- * overlap on the GPU (different streams, or threads) race.  Validates A and
- * waits for the verdict, then runs asynchronously on `stream`. */
+ * It runs on the current device, and A and the outputs must live there (a
+ * buffer on another GPU: SPG_ERR_INVALID_ARG).  The first call on each device
+ * resolves that array's address (set-up) and keeps it; make that first call
+ * before any stream capture, and do not use the library across a
+ * cudaDeviceReset of the device.  All calls share the array: calls that
+ * overlap on the GPU (different streams, or threads) race.  Every call first
+ * validates A on `stream` and waits there for the verdict (a device-to-host
+ * copy and a stream synchronisation), then runs the transpose asynchronously
+ * on `stream`. */
 spg_status spg_transpose_noalloc(const spg_csr_dev* A, int32_t* t_rowptr, int32_t* t_col,
                                  double* t_val, void* stream);
 

@@ -39,6 +39,9 @@ def test_server_results_equal_standalone_and_oracle():
         assert st["completed"] == len(mats) and st["rejected"] == 0
         assert st["batches"] >= 1 and any(inf["batched"] for inf in infos)
         assert st["p99_ms"] >= st["p50_ms"] > 0
+        for inf in infos:
+            assert inf["submit_ms"] <= inf["start_ms"] <= inf["planned_ms"] <= inf["run_ms"]
+            assert inf["run_ms"] <= inf["done_ms"]
         with Engine("cuda:0") as eng:
             for i, (A, d, t, rid) in enumerate(zip(mats, ds, tasks, ids)):
                 got = srv.result(rid)
@@ -150,3 +153,64 @@ def test_close_with_a_request_waiting_for_budget():
     with pytest.raises(_capi.SpgemmError):
         srv.wait(r2, timeout_ms=1000)
     srv.close()
+
+
+def workspace_bound(eng, As, task, batched):
+    import ctypes
+    from appt_spgemm_b200._capi import SpgCsrDev, check, lib
+    arr = (SpgCsrDev * len(As))(*[A.struct() for A in As])
+    out = ctypes.c_int64()
+    check(lib().spg_plan_workspace_bound(eng._h, _capi.TASKS[task], len(As), arr,
+                                         1 if batched else 0, ctypes.byref(out)), "bound")
+    return out.value
+
+
+def test_plan_workspace_bound_covers_every_plan():
+    """The host-side bound a budgeted caller reserves before planning is at
+    least the workspace the plan then holds, single and batched, for every
+    task, heavy rows and the windowed heavy kernel included."""
+    from appt_spgemm_b200.engine import Engine
+    mats, _ = request_mix()
+    mats = mats + [csr.erdos_renyi(1 << 14, 80.0, 9), csr.rmat(14, 16, seed=11)]
+    with Engine("cuda:0") as eng:
+        ds = [dev(A) for A in mats]
+        for task in ("AA", "AAt", "AAtS"):
+            for d in ds:
+                p = eng.plan(d, task)
+                assert workspace_bound(eng, [d], task, False) >= p.info["workspace_bytes"], task
+                p.close()
+            p = eng.plan_batched(ds[:6], task)
+            assert workspace_bound(eng, ds[:6], task, True) >= p.info["workspace_bytes"], task
+            p.close()
+
+
+def test_server_holds_at_most_its_budget():
+    """Several large requests at once under a budget of about two and a half of
+    them: plans are only made once their workspace bound is reserved, a job
+    that cannot run yet holds nothing, so the bytes the server actually holds
+    (plans, execute workspace, results) never exceed the budget; every request
+    still completes, equal to its standalone product."""
+    from appt_spgemm_b200.engine import Engine, Server
+    big = csr.stencil27(40, 8)
+    d = dev(big)
+    with Engine("cuda:0") as eng:
+        p = eng.plan(d, "AA")
+        need = (p.info["workspace_bytes"] + p.info["exec_workspace_bytes"] +
+                p.info["output_bytes"])
+        bound = workspace_bound(eng, [d], "AA", False)
+        p.close()
+        alone = eng.multiply(d, "AA").to_host()
+    budget = int(max(need, bound) * 2.5)
+    with Server(workers=3, memory_budget_bytes=budget, batch_rows=1) as srv:
+        ids = [srv.submit(d, "AA") for _ in range(6)]
+        for rid in ids:
+            assert srv.wait(rid, 120000)["status"] == _capi.SPG_OK
+            got = srv.result(rid).to_host()
+            for x, y in zip(got, alone):
+                assert np.array_equal(x.view(np.uint8), y.view(np.uint8))
+            srv.release(rid)
+        st = srv.stats()
+        assert st["completed"] == 6 and st["rejected"] == 0
+        assert 0 < st["peak_held_bytes"] <= budget
+        assert st["peak_held_bytes"] <= st["peak_reserved_bytes"] <= budget
+        assert st["held_bytes"] == 0 and st["reserved_bytes"] == 0

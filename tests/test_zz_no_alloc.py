@@ -59,9 +59,34 @@ def test_noalloc_transpose_matches_allocating_entry_point():
         assert np.array_equal(got[2].view(np.int64), want[2].view(np.int64))  # bit-exact
 
 
+def test_noalloc_at_its_limits_and_empty():
+    # n = 65,536 rows and nnz = 524,288 entries use the whole static scratch;
+    # then matrices with no entries, and one with no rows
+    cases = [csr.uniform(65536, 8, seed=43),
+             csr.CsrHost(5, np.zeros(6, np.int32), np.zeros(0, np.int32), np.zeros(0)),
+             csr.CsrHost(0, np.zeros(1, np.int32), np.zeros(0, np.int32), np.zeros(0))]
+    assert cases[0].n == 65536 and cases[0].nnz == 524288
+    for A in cases:
+        for _ in range(2):
+            got = transpose_noalloc(A)
+            want = transpose_allocating(A)
+            assert np.array_equal(got[0], want[0])
+            assert np.array_equal(got[1], want[1])
+            assert np.array_equal(got[2].view(np.int64), want[2].view(np.int64))
+
+
 def test_noalloc_refuses_inputs_beyond_its_scratch():
+    # one row too many
     n = 65537
     A = csr.CsrHost(n, np.zeros(n + 1, np.int32), np.zeros(0, np.int32), np.zeros(0))
+    with pytest.raises(SpgemmError) as e:
+        transpose_noalloc(A)
+    assert e.value.status == _capi.SPG_ERR_UNSUPPORTED
+    # one entry too many (refused on its sizes, before anything runs)
+    n, nnz = 65536, 524289
+    rp = np.full(n + 1, nnz, np.int32)
+    rp[0] = 0
+    A = csr.CsrHost(n, rp, np.zeros(nnz, np.int32), np.zeros(nnz))
     with pytest.raises(SpgemmError) as e:
         transpose_noalloc(A)
     assert e.value.status == _capi.SPG_ERR_UNSUPPORTED
