@@ -54,7 +54,8 @@ class SpgConfig(Structure):
                 ("window_bits", c_int32), ("force_heavy", c_int32), ("sym_load_pct", c_int32),
                 ("num_load_pct", c_int32), ("heavy_split", c_int32),
                 ("pool_release_bytes", c_int64), ("heavy_block_budget", c_int64),
-                ("grid_sms", c_int64), ("reserved", c_int64 * 3)]
+                ("grid_sms", c_int64), ("small_max_nnz", c_int64), ("heavy_vcap", c_int64),
+                ("reserved", c_int64 * 1)]
 
 
 class SpgEngResult(Structure):
@@ -144,6 +145,7 @@ SIGNATURES = {
     "spg_get_config": (c_int32, [_ctx_p, POINTER(SpgConfig)]),
     "spg_autotune": (c_int32, [_ctx_p, c_int32, c_int32, POINTER(SpgCsrDev), c_int32,
                                POINTER(SpgConfig), c_void_p]),
+    "spg_autotune_trials": (c_int32, [_ctx_p, POINTER(c_int32), POINTER(c_int32)]),
     "spg_profile_enable": (c_int32, [_ctx_p, c_int32]),
     "spg_profile_reset": (c_int32, [_ctx_p]),
     "spg_profile_read": (c_int32, [_ctx_p, c_char_p, c_uint64]),

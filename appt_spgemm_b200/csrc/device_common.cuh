@@ -91,6 +91,54 @@ __device__ __forceinline__ void insert_acc(int* keys, double* vals, int j, doubl
   }
 }
 
+// Insert of one segment by a whole warp that owns the table (every lane
+// calls; lanes without a key pass j < 0).  Slots are claimed without shared
+// atomics: in each round every pending lane reads its slot; the lanes that see
+// an empty slot are grouped by slot (__match_any_sync) and the lowest lane of
+// each group writes its key there; lanes that see their own key are done;
+// lanes that see another key move to the next slot; the other lanes of a group
+// read the same slot again in the next round (it may now hold their key).  No
+// other warp touches the table, so a __syncwarp between a round's reads and its
+// writes and one after the writes order every access.  NUMERIC: a claimed
+// slot's value becomes 0.0 + v and a found slot's value slot + v (the keys of
+// one call are distinct, so no two lanes write one value; the closing
+// __syncwarp keeps the k order between calls).  A table that stays full for
+// 2T + 2 rounds is reported, never spun on.
+template <int LOG2T, bool NUMERIC>
+__device__ __forceinline__ void warp_insert(int* keys, double* vals, int j, double v,
+                                            uint32_t* status) {
+  constexpr unsigned T = 1u << LOG2T;
+  const unsigned lane_bit = 1u << (threadIdx.x & 31);
+  unsigned h = hash_slot<LOG2T>(j);
+  bool pending = j >= 0;
+#pragma unroll 1
+  for (unsigned round = 0; __any_sync(0xffffffffu, pending); ++round) {
+    if (round > 2 * T + 1) {
+      if (pending) report(status, DEV_ERR_HASH_FULL);
+      break;
+    }
+    const int cur = pending ? keys[h] : 0;
+    const bool found = pending && cur == j;
+    const bool empty = pending && cur == kEmptyKey;
+    const unsigned em = __ballot_sync(0xffffffffu, empty);
+    bool win = false;
+    if (empty) {
+      const unsigned grp = __match_any_sync(em, h);
+      win = (grp & (0u - grp)) == lane_bit;
+    }
+    __syncwarp();
+    if (win) {
+      keys[h] = j;
+      if (NUMERIC) vals[h] = __dadd_rn(0.0, v);
+    } else if (NUMERIC && found) {
+      vals[h] = __dadd_rn(vals[h], v);
+    }
+    if (win || found) pending = false;
+    else if (pending && !empty) h = (h + 1) & (T - 1);
+    __syncwarp();
+  }
+}
+
 // ---- lane groups -------------------------------------------------------------
 // A row is processed by a group of G lanes: a power-of-two slice of one warp
 // (G <= 32, several rows per CTA) or the whole CTA (G = blockDim.x > 32).

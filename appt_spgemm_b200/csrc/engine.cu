@@ -44,6 +44,7 @@ struct spg_ctx {
   bool prof = false;
   std::vector<ProfEntry> pending;
   std::map<std::string, std::pair<double, long long>> prof_acc;
+  int32_t tune_timed = 0, tune_pruned = 0;  // the last spg_autotune's candidates
   std::vector<cudaEvent_t> event_pool;
   long long launch_base = 0;
 };
@@ -144,6 +145,10 @@ struct spg_plan {
   uint16_t* blk_cnt = nullptr;
   int blk_log2 = 12;
   bool heavy_windows = false;  // the windowed heavy kernel runs: execute takes its cursors
+  // one-readback plan: every row in one warp-per-row launch per phase, the
+  // numeric one with tables of 2^small_log2 slots
+  bool small = false;
+  int small_log2 = 6;
   int32_t* hqueue = nullptr;  // next row of the CTA-per-row kernels (zeroed before each launch)
   int window_bits = 1 << 20;  // heavy-path shape (heavy_shape)
   int heavy_threads = 1024;
@@ -196,6 +201,14 @@ spg_status status_from_bits(uint32_t bits) {
   return set_error(SPG_ERR_CUDA, "device status word 0x%x", bits);
 }
 
+// The one-readback plan takes A·A and A·Aᵀ of matrices up to these sizes.
+constexpr int64_t kSmallMaxNnzDefault = (int64_t)1 << 20;
+constexpr int32_t kSmallMaxN = 65536;
+// Its symbolic table (2^11 slots per warp) holds rows of up to this many
+// products at 75% load; a larger row sends the plan to the regular path.
+constexpr int kSmallSymLog2 = 11;
+constexpr int64_t kSmallCap = 1536;
+
 spg_config merged_config(const spg_config* user) {
   spg_config c{};
   if (user && user->struct_size >= (int32_t)sizeof(int32_t)) {
@@ -222,6 +235,12 @@ spg_config merged_config(const spg_config* user) {
   if (c.heavy_block_budget <= 0) c.heavy_block_budget = (int64_t)1 << 27;  // 256 MB of counts
   if (c.grid_sms < 0) c.grid_sms = 0;
   if (c.grid_sms > (1 << 16)) c.grid_sms = 1 << 16;
+  if (c.small_max_nnz == 0) c.small_max_nnz = kSmallMaxNnzDefault;
+  if (c.heavy_vcap > 0) {  // a power of two in [1024, 16384]
+    int64_t v = 1024;
+    while (v * 2 <= c.heavy_vcap && v < 16384) v *= 2;
+    c.heavy_vcap = v;
+  }
   return c;
 }
 
@@ -369,6 +388,159 @@ void plan_free(spg_plan* p) {
   }
   for (void* ptr : p->ptrs) cudaFreeAsync(ptr, p->stream);
   delete p;
+}
+
+// The plan of a small A·A or A·Aᵀ with one host synchronisation.  The regular
+// plan waits three times (validation verdict, bin sizes, nnz(C)); on a
+// matrix of a few thousand rows those round trips and the per-bin launches
+// are most of the call.  Here every kernel runs before the verdict is known
+// (the pre-pass and the transpose check every index they use; a row with an
+// invalid index gets f = −1 and is skipped), every row takes one
+// warp-per-row symbolic launch with a 2048-slot table, and one readback
+// brings the verdict, nnz(C) and the row statistics together.  A·Aᵀ always
+// uses the counting-sort transpose (no symmetric-pattern shortcut, which would
+// need the verdict first).  A row of more than kSmallCap products reports
+// DEV_ERR_SMALL_CAP, and the caller plans again on the regular path
+// (*fallback).  Execute then runs one numeric launch over all rows.
+spg_status plan_build_small(spg_plan* p, const spg_csr_dev* Ad, bool* fallback) {
+  *fallback = false;
+  spg_ctx* ctx = p->ctx;
+  cudaStream_t st = p->stream;
+  const int32_t n = Ad->n;
+  const int64_t nnz = Ad->nnz;
+  const bool aat = p->task == SPG_TASK_AAT;
+  p->small = true;
+  p->n = n;
+  p->A = MatView{n, nnz, Ad->rowptr, Ad->col, Ad->val};
+  p->info.n = n;
+  p->info.task = p->task;
+  p->info.nnz_a = nnz;
+  // one allocation, carved into 256-byte aligned pieces
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t o = off;
+    off += (bytes + 255) & ~(size_t)255;
+    return o;
+  };
+  const size_t nn = (size_t)(n > 0 ? n : 1), nz = (size_t)(nnz > 0 ? nnz : 1);
+  const size_t o_f = take(8 * nn), o_lo = take(4 * nn), o_hi = take(4 * nn),
+               o_cnt = take(4 * nn), o_rp = take(8 * (nn + 1)), o_scan = take(scan_tmp_bytes(n)),
+               o_stats = take(32), o_q = take(4);
+  size_t o_bp = 0, o_bi = 0, o_bx = 0, o_tc = 0, o_tu = 0, o_ts = 0, o_tk = 0, o_tv = 0,
+         o_ll = 0, o_lc = 0;
+  if (aat) {
+    o_bp = take(4 * (nn + 1));
+    o_bi = take(4 * nz);
+    o_bx = take(8 * nz);
+    o_tc = take(4 * nn);
+    o_tu = take(4 * nn);
+    o_ts = take(scan_tmp_bytes(n));
+    o_tk = take(4 * nz);
+    o_tv = take(8 * nz);
+    o_ll = take(4 * nn);
+    o_lc = take(4);
+  }
+  char* w = nullptr;
+  TRY(palloc(p, &w, (int64_t)off));
+  p->f = (int64_t*)(w + o_f);
+  p->lo = (int32_t*)(w + o_lo);
+  p->hi = (int32_t*)(w + o_hi);
+  p->rownnz = (int32_t*)(w + o_cnt);
+  p->rowptr = (int64_t*)(w + o_rp);
+  p->hqueue = (int32_t*)(w + o_q);
+  unsigned long long* stats = (unsigned long long*)(w + o_stats);
+  TRY_CUDA(cudaMemsetAsync(ctx->d_status, 0, 2 * sizeof(uint32_t), st), "status reset");
+  {
+    ProfScope ps(ctx, "plan/validate", st);
+    TRY_CUDA(launch_validate(p->A, ctx->d_status, st), "validate");
+  }
+  if (aat) {
+    TransposeWork tw{};
+    tw.cnt = (int32_t*)(w + o_tc);
+    tw.cursor = (int32_t*)(w + o_tu);
+    tw.scan_tmp = (void*)(w + o_ts);
+    tw.tmp_col = (int32_t*)(w + o_tk);
+    tw.tmp_val = (double*)(w + o_tv);
+    tw.long_list = (int32_t*)(w + o_ll);
+    tw.long_count = (int32_t*)(w + o_lc);
+    tw.status = ctx->d_status;
+    p->bt_rowptr = (int32_t*)(w + o_bp);
+    p->bt_col = (int32_t*)(w + o_bi);
+    p->bt_val = (double*)(w + o_bx);
+    // slots an invalid input leaves unwritten hold column 0, so the row sort
+    // stays in range; the plan then fails on the verdict
+    TRY_CUDA(cudaMemsetAsync(tw.tmp_col, 0, 4 * nz, st), "memset");
+    ProfScope ps(ctx, "plan/transpose", st);
+    TRY_CUDA(launch_transpose(p->A, p->bt_rowptr, p->bt_col, p->bt_val, tw, ctx->num_sms, st),
+             "transpose");
+    p->tw = tw;
+    p->B = MatView{n, nnz, p->bt_rowptr, p->bt_col, p->bt_val};
+  } else {
+    p->B = p->A;
+  }
+  {
+    ProfScope ps(ctx, "plan/prepass", st);
+    TRY_CUDA(launch_prepass(p->A, p->B, p->f, p->lo, p->hi, st), "prepass");
+  }
+  RowArgs ra{};
+  ra.A = p->A;
+  ra.B = p->B;
+  ra.rows = nullptr;
+  ra.nrows = n;
+  ra.G = 32;
+  ra.rownnz = p->rownnz;
+  ra.status = ctx->d_status;
+  ra.lo = p->lo;
+  ra.hi = p->hi;
+  ra.fsmall = p->f;
+  ra.fcap = kSmallCap;
+  if (n > 0) {
+    ProfScope ps(ctx, "sym/small", st);
+    TRY_CUDA(launch_hash_w32(kSmallSymLog2, false, false, ra, ctx->num_sms, st), "symbolic");
+  }
+  {
+    ProfScope ps(ctx, "plan/scan", st);
+    TRY_CUDA(launch_scan_i32_i64(p->rownnz, p->rowptr, n, w + o_scan, st), "row pointer scan");
+  }
+  TRY_CUDA(launch_row_stats(p->f, p->rownnz, n, stats, st), "row stats");
+  int64_t* hp = ctx->h_pin;
+  TRY_CUDA(cudaMemcpyAsync(hp, ctx->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, st),
+           "readback");
+  TRY_CUDA(cudaMemcpyAsync(hp + 1, p->rowptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st),
+           "readback");
+  TRY_CUDA(cudaMemcpyAsync(hp + 2, stats, sizeof(unsigned long long) * 3, cudaMemcpyDeviceToHost,
+                           st), "readback");
+  TRY_CUDA(cudaStreamSynchronize(st), "plan sync");
+  const uint32_t bits = *(const uint32_t*)hp;
+  if (bits & DEV_ERR_INVALID_CSR) return status_from_bits(DEV_ERR_INVALID_CSR);
+  if (bits & DEV_ERR_SMALL_CAP) {
+    *fallback = true;
+    return SPG_OK;
+  }
+  TRY(status_from_bits(bits));
+  const unsigned long long* sv = (const unsigned long long*)(hp + 2);
+  p->nnz_c = n > 0 ? hp[1] : 0;
+  p->info.nnz_c = p->nnz_c;
+  p->info.products = (int64_t)sv[0];
+  p->info.products_computed = (int64_t)sv[0];
+  p->info.max_row_products = (int64_t)sv[1];
+  p->info.max_row_nnz = (int64_t)sv[2];
+  p->info.heavy_rows = 0;
+  p->info.bins_used = 1;
+  p->info.symmetric_pattern = 0;
+  // numeric table: the exact largest row at the numeric load, 64 to 2048 slots
+  int lg = ceil_log2_64((int64_t)sv[2] * 100 / ctx->cfg.num_load_pct + 1);
+  p->small_log2 = lg < 6 ? 6 : (lg > 11 ? 11 : lg);
+  p->info.output_bytes = 8 * ((int64_t)n + 1) + 12 * p->nnz_c;
+  p->info.workspace_bytes = p->ws_bytes;
+  p->info.exec_workspace_bytes = 0;
+  return SPG_OK;
+}
+
+bool small_plan_eligible(const spg_ctx* ctx, spg_task task, const spg_csr_dev* A) {
+  const spg_config& c = ctx->cfg;
+  return (task == SPG_TASK_AA || task == SPG_TASK_AAT) && c.small_max_nnz > 0 &&
+         A->nnz <= c.small_max_nnz && A->n <= kSmallMaxN && !c.force_heavy;
 }
 
 spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
@@ -679,6 +851,15 @@ spg_status execute_impl(spg_plan* p, spg_csr_out* C, cudaStream_t st) {
       ra.lcol = (int32_t*)lc;
       ra.lval = (double*)lv;
     }
+    if (p->small && n > 0) {
+      RowArgs r = ra;
+      r.rows = nullptr;
+      r.nrows = n;
+      r.G = 32;
+      ProfScope ps(ctx, "num/small", st);
+      cudaError_t e = launch_hash_w32(p->small_log2, true, false, r, ctx->num_sms, st);
+      if (e != cudaSuccess) result = cuda_status(e, "numeric");
+    }
     for (int b = 1; b <= kNumTableBins && result == SPG_OK; ++b) {
       if (p->num_count[b] == 0) continue;
       RowArgs r = ra;
@@ -717,11 +898,19 @@ spg_status execute_impl(spg_plan* p, spg_csr_out* C, cudaStream_t st) {
       h.f = p->f;
       h.split = !windows ? 0
                 : ctx->cfg.heavy_split > 0 ? (int64_t)ctx->cfg.heavy_split : kHeavySplitDefault;
+      // CTA rows: values in shared memory window by window when the block
+      // counts and cursors exist and the configuration allows it
+      const bool shared_values = windows && ctx->cfg.heavy_vcap >= 0;
+      const int win_threads = ctx->cfg.heavy_threads > 512 ? 1024 : 512;
+      h.vcap = ctx->cfg.heavy_vcap > 0 ? (int32_t)ctx->cfg.heavy_vcap
+                                       : (win_threads > 512 ? 16384 : 8192);
+      h.wcap_bits = win_threads > 512 ? (1 << 18) : (1 << 17);
       ProfScope ps(ctx, "num/heavy", st);
       cudaError_t e = cudaSuccess;
       if (windows) e = launch_heavy_w32(gram, h, ctx->num_sms, st);
       if (e == cudaSuccess)
-        e = launch_heavy(true, gram, h, p->heavy_threads, ctx->num_sms, st);
+        e = shared_values ? launch_heavy_win(gram, h, win_threads, ctx->num_sms, st)
+                          : launch_heavy(true, gram, h, p->heavy_threads, ctx->num_sms, st);
       if (e != cudaSuccess) { result = cuda_status(e, "numeric heavy"); break; }
     }
     if (gram && p->nnz_low > 0) {
@@ -855,7 +1044,22 @@ spg_status spg_plan_create(spg_ctx* ctx, spg_task task, const spg_csr_dev* A, vo
   p->ctx = ctx;
   p->task = task;
   p->stream = (cudaStream_t)stream;
-  spg_status st = plan_build(p, A);
+  spg_status st = SPG_OK;
+  bool regular = true;
+  if (small_plan_eligible(ctx, task, A)) {
+    bool fallback = false;
+    st = plan_build_small(p, A, &fallback);
+    if (st == SPG_OK && fallback) {  // a row beyond the small table: plan again
+      plan_free(p);
+      p = new spg_plan();
+      p->ctx = ctx;
+      p->task = task;
+      p->stream = (cudaStream_t)stream;
+    } else {
+      regular = false;
+    }
+  }
+  if (regular) st = plan_build(p, A);
   if (st != SPG_OK) {
     // keep the message of the failure, then release what was allocated
     cudaStreamSynchronize(p->stream);
@@ -1138,9 +1342,34 @@ spg_status spg_autotune(spg_ctx* ctx, spg_task task, int32_t count, const spg_cs
     *out = v[v.size() / 2];
     return SPG_OK;
   };
+  // Structural features of the input, as the reference's dispatcher reads
+  // them (bench/dispatch.cu:26-38), computed on the device: for a batch, the
+  // mean degree over all instances and the largest row / column degree.
+  int64_t tot_n = 0, tot_nnz = 0;
+  int32_t max_deg = 0, max_col = 0;
+  for (int32_t b = 0; b < count; ++b) {
+    spg_descriptors d{};
+    spg_status ds = spg_describe(ctx, &As[b], &d, stream);
+    if (ds != SPG_OK) {
+      ctx->cfg = start;
+      return ds;
+    }
+    tot_n += d.n;
+    tot_nnz += d.nnz;
+    max_deg = std::max(max_deg, d.max_deg);
+    max_col = std::max(max_col, d.max_col_deg);
+  }
+  const double mean_deg = tot_n > 0 ? (double)tot_nnz / (double)tot_n : 1.0;
+  // B rows are A's rows (A·A) or its columns (A·Aᵀ)
+  const int64_t max_b = task == SPG_TASK_AA ? max_deg : max_col;
+  // a row has at most max_deg · max_b products, so at most that many entries
+  const int64_t max_row = (int64_t)max_deg * max_b;
+  ctx->tune_timed = 0;
+  ctx->tune_pruned = 0;
   spg_config cur = start;
   float cur_ms = 0.f;
   spg_status s = measure(cur, &cur_ms);
+  ++ctx->tune_timed;
   if (s != SPG_OK) {
     ctx->cfg = start;
     return s;
@@ -1161,13 +1390,38 @@ spg_status spg_autotune(spg_ctx* ctx, spg_task task, int32_t count, const spg_cs
       {&spg_config::window_bits, {1 << 18, 1 << 19, 1 << 20}, true},
       {&spg_config::heavy_split, {1, 32, 128, 512, 1 << 30}, true},
   };
+  // Candidates the features rule out are not timed:
+  //  - lanes per row of the sub-warp bins: only the powers of two next to the
+  //    mean B-row length (a group much wider idles, much narrower serialises);
+  //  - the shared-table cap: only when some row can need a table above 2048
+  //    slots (max_row entries at the numeric load);
+  //  - the heavy-path knobs: only when the plan has heavy rows;
+  //  - a single matrix that the one-readback plan takes whole (no row above
+  //    its table) runs no binned kernel: only the numeric load matters.
+  const bool one_readback = count == 1 && small_plan_eligible(ctx, task, &As[0]) &&
+                            max_row <= kSmallCap;
+  int near_lanes = 4;
+  while (near_lanes < 32 && near_lanes < mean_deg) near_lanes <<= 1;
+  const bool big_tables = max_row * 100 / std::max(20, (int)cur.num_load_pct) + 1 > 2048;
+  auto pruned = [&](const Knob& k, int32_t v) {
+    if (k.heavy_only && !has_heavy) return true;
+    if (one_readback && k.field != &spg_config::num_load_pct) return true;
+    if (k.field == &spg_config::lanes_per_row)
+      return v != near_lanes && v != near_lanes / 2 && v != near_lanes * 2;
+    if (k.field == &spg_config::max_smem_slots) return !big_tables;
+    return false;
+  };
   for (const Knob& k : knobs) {
-    if (k.heavy_only && !has_heavy) continue;
     for (int32_t v : k.values) {
       if (cur.*(k.field) == v) continue;
+      if (pruned(k, v)) {
+        ++ctx->tune_pruned;
+        continue;
+      }
       spg_config c = cur;
       c.*(k.field) = v;
       float t = 0.f;
+      ++ctx->tune_timed;
       if (measure(c, &t) != SPG_OK) continue;  // a candidate that fails is skipped
       if (t < cur_ms * 0.98f) {
         cur = merged_config(&c);
@@ -1179,6 +1433,14 @@ spg_status spg_autotune(spg_ctx* ctx, spg_task task, int32_t count, const spg_cs
   ctx->cfg.device = start.device;
   if (best) *best = ctx->cfg;
   begin_call();
+  return SPG_OK;
+}
+
+spg_status spg_autotune_trials(const spg_ctx* ctx, int32_t* timed, int32_t* pruned) {
+  begin_call();
+  if (!ctx || !timed || !pruned) return set_error(SPG_ERR_INVALID_ARG, "null argument");
+  *timed = ctx->tune_timed;
+  *pruned = ctx->tune_pruned;
   return SPG_OK;
 }
 

@@ -21,6 +21,7 @@ enum DeviceErrorBits : uint32_t {
   DEV_ERR_OVERFLOW = 1u << 1,   // a row wrote more entries than the symbolic phase counted
   DEV_ERR_BAD_INDEX = 1u << 2,  // a column index outside [0, n) was met
   DEV_ERR_INVALID_CSR = 1u << 3,  // input CSR failed validation
+  DEV_ERR_SMALL_CAP = 1u << 4,    // a row exceeds the one-readback plan's table (replan)
 };
 
 // ---- engine constants ------------------------------------------------------

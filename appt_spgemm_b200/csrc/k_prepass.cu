@@ -51,18 +51,32 @@ cudaError_t launch_validate(const MatView& A, uint32_t* status, cudaStream_t s) 
 // ---------------------------------------------------------------------------
 // pre-pass: products and output column span per row (one warp per row)
 // ---------------------------------------------------------------------------
+// Every index is checked before it is used, so the kernel may run before the
+// host has seen the validation verdict (the one-readback plan): a row that
+// meets a row pointer or column outside its range gets f = −1, and the later
+// kernels of that plan skip it.
 __global__ void k_prepass(MatView A, MatView B, int64_t* __restrict__ f, int32_t* __restrict__ lo,
                           int32_t* __restrict__ hi) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t i = warp; i < A.n; i += nwarps) {
-    const int32_t s = A.rowptr[i], e = A.rowptr[i + 1];
+    int32_t s = A.rowptr[i], e = A.rowptr[i + 1];
+    bool bad = s < 0 || e < s || (int64_t)e > A.nnz;
+    if (bad) s = e = 0;
     long long prod = 0;
     int mn = INT_MAX, mx = -1;
     for (int32_t p = s + lane; p < e; p += 32) {
       const int32_t k = A.col[p];
+      if (k < 0 || k >= B.n) {
+        bad = true;
+        continue;
+      }
       const int32_t bs = B.rowptr[k], be = B.rowptr[k + 1];
+      if (bs < 0 || be < bs || (int64_t)be > B.nnz) {
+        bad = true;
+        continue;
+      }
       if (be > bs) {
         prod += be - bs;
         mn = min(mn, B.col[bs]);
@@ -74,10 +88,11 @@ __global__ void k_prepass(MatView A, MatView B, int64_t* __restrict__ f, int32_t
       mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
       mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     }
+    bad = __any_sync(0xffffffffu, bad);
     if (lane == 0) {
-      f[i] = prod;
-      lo[i] = mn;
-      hi[i] = mx;
+      f[i] = bad ? -1 : prod;
+      lo[i] = bad ? INT_MAX : mn;
+      hi[i] = bad ? -1 : mx;
     }
   }
 }
@@ -302,8 +317,10 @@ cudaError_t launch_scan_i32_i32(const int32_t* in, int32_t* out, int64_t n, void
 // ---------------------------------------------------------------------------
 __global__ void k_col_count(MatView A, int32_t* __restrict__ cnt) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < A.nnz; p += stride)
-    atomicAdd(&cnt[A.col[p]], 1);
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < A.nnz; p += stride) {
+    const int32_t k = A.col[p];
+    if (k >= 0 && k < A.n) atomicAdd(&cnt[k], 1);  // others: invalid input, never counted
+  }
 }
 
 cudaError_t launch_col_count(const MatView& A, int32_t* cnt, cudaStream_t s) {

@@ -29,6 +29,12 @@ namespace spg {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
+#ifndef SPG_W32_CAS
+#define SPG_W32_CAS 0
+#endif
+// 1: the CAS-first probe (insert_acc) per lane; 0: warp_insert's atomic-free
+// claims.
+constexpr bool kCasInsert = SPG_W32_CAS != 0;
 // Rows of more entries than this sort with the radix sort rather than the
 // register bitonic network (whose 8-per-lane form costs about 1,000 warp
 // instructions a row against about 600 for two or three digit passes).
@@ -146,7 +152,18 @@ __global__ void __launch_bounds__(256, 5) k_hash_w32(RowArgs a) {
   int* keys = (int*)(base_p + (NUMERIC ? (size_t)T * 8 : 0));
 
   for (int r = blockIdx.x * nw + w; r < a.nrows; r += gridDim.x * nw) {
-    const int row = a.rows[r];
+    const int row = a.rows ? a.rows[r] : r;
+    if (!NUMERIC && a.fsmall) {
+      const int64_t fr = a.fsmall[row];
+      if (fr < 0 || fr > a.fcap) {
+        if (lane == 0) {
+          if (fr > a.fcap) report(a.status, DEV_ERR_SMALL_CAP);
+          a.rownnz[row] = 0;
+          if (GRAM) a.rowlow[row] = 0;
+        }
+        continue;
+      }
+    }
     for (int s = lane * 4; s < T; s += 128) *(int4*)(keys + s) = make_int4(-1, -1, -1, -1);
     __syncwarp();
     const int32_t ps = a.A.rowptr[row], pe = a.A.rowptr[row + 1];
@@ -180,10 +197,14 @@ __global__ void __launch_bounds__(256, 5) k_hash_w32(RowArgs a) {
 #pragma unroll
           for (int d = 0; d < D; ++d) {
             const int j = jr[d];
-            if (j >= 0 && !(NUMERIC && GRAM && j < row))
-              insert_acc<LOG2T, NUMERIC>(keys, vals, j, NUMERIC ? __dmul_rn(ar[d], br[d]) : 0.0,
-                                         a.status);
-            if (NUMERIC) __syncwarp();  // k-order of the accumulation
+            const bool use = j >= 0 && !(NUMERIC && GRAM && j < row);
+            const double p = NUMERIC ? __dmul_rn(ar[d], br[d]) : 0.0;
+            if (kCasInsert) {
+              if (use) insert_acc<LOG2T, NUMERIC>(keys, vals, j, p, a.status);
+              if (NUMERIC) __syncwarp();  // k-order of the accumulation
+            } else {
+              warp_insert<LOG2T, NUMERIC>(keys, vals, use ? j : -1, p, a.status);
+            }
           }
         }
         continue;
@@ -229,10 +250,14 @@ __global__ void __launch_bounds__(256, 5) k_hash_w32(RowArgs a) {
 #pragma unroll
         for (int d = 0; d < D; ++d) {
           const int j = jr[d];
-          if (j >= 0 && !(NUMERIC && GRAM && j < row))
-            insert_acc<LOG2T, NUMERIC>(keys, vals, j, NUMERIC ? __dmul_rn(ar[d], br[d]) : 0.0,
-                                       a.status);
-          if (NUMERIC) __syncwarp();  // k-order of the accumulation
+          const bool use = j >= 0 && !(NUMERIC && GRAM && j < row);
+          const double p = NUMERIC ? __dmul_rn(ar[d], br[d]) : 0.0;
+          if (kCasInsert) {
+            if (use) insert_acc<LOG2T, NUMERIC>(keys, vals, j, p, a.status);
+            if (NUMERIC) __syncwarp();  // k-order of the accumulation
+          } else {
+            warp_insert<LOG2T, NUMERIC>(keys, vals, use ? j : -1, p, a.status);
+          }
         }
       }
     }

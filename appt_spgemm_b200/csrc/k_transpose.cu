@@ -21,10 +21,15 @@ __global__ void k_transpose_scatter(MatView A, const int32_t* __restrict__ t_row
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t i = warp; i < A.n; i += nwarps) {
-    const int32_t s = A.rowptr[i], e = A.rowptr[i + 1];
+    int32_t s = A.rowptr[i], e = A.rowptr[i + 1];
+    // indices are checked (the one-readback plan runs this before the host has
+    // the validation verdict): an invalid input only leaves slots unwritten
+    if (s < 0 || e < s || (int64_t)e > A.nnz) s = e = 0;
     for (int32_t p = s + lane; p < e; p += 32) {
       const int32_t k = A.col[p];
+      if (k < 0 || k >= A.n) continue;
       const int32_t d = t_rowptr[k] + atomicAdd(&cursor[k], 1);
+      if (d >= t_rowptr[k + 1]) continue;
       tmp_col[d] = (int32_t)i;
       tmp_val[d] = A.val[p];
     }

@@ -110,7 +110,7 @@ cudaError_t launch_scan_i32_i32(const int32_t* in, int32_t* out, int64_t n, void
 
 struct RowArgs {
   MatView A, B;
-  const int32_t* rows;      // this bin's rows
+  const int32_t* rows;      // this bin's rows (nullptr: rows 0..nrows-1)
   int32_t nrows;
   int32_t G;                // lanes per row (warp bins); CTA bins use blockDim
   // symbolic outputs
@@ -137,6 +137,12 @@ struct RowArgs {
   // CTA-per-row bins: in a persistent launch rows are drawn from this counter
   // (zeroed by the launcher) as CTAs free up; nullptr: dealt out in turn
   int32_t* queue;
+  // the one-readback plan's symbolic launch (warp kernels): rows whose
+  // pre-pass product count is negative (an invalid index met) or above fcap
+  // (beyond the table) are skipped with a zero count, the latter reported as
+  // DEV_ERR_SMALL_CAP; nullptr: every row is processed
+  const int64_t* fsmall;
+  int64_t fcap;
 };
 
 // Writes m sorted packed words ((col − lo) << LOG2T | slot) as a row's columns
@@ -210,6 +216,8 @@ struct HeavyArgs {
   int32_t cap;              // numeric: most distinct columns per window
   int32_t sub_log2;         // numeric: window width inside a block above cap
   int4* hcur;               // numeric: per entry of A {B cursor, B row end, next column, 0}
+  int32_t vcap;             // shared-value CTA kernel: most values per window
+  int32_t wcap_bits;        // shared-value CTA kernel: widest window (bitmap bits)
   // numeric: rows fed by many short B rows (mean length below `split`) take
   // the windowed warp kernel, rows dominated by long B rows the CTA kernel,
   // whose 1024 threads stream each long B row (each kernel skips the other's
@@ -239,6 +247,12 @@ size_t heavy_smem_bytes(bool numeric, int threads, int window_bits);
 // blk_off[0..n] (launch_scan_i32_i64 with tmp of scan_tmp_bytes(n)).
 cudaError_t launch_heavy_blocks(const BinSource& bsym, int blk_log2, int32_t* nblk,
                                 int64_t* blk_off, void* scan_tmp, cudaStream_t s);
+
+// Numeric phase of the CTA rows with their values in shared memory, window by
+// window (k_heavy_win.cu); needs blk_cnt, hcur and queue.
+cudaError_t launch_heavy_win(bool gram, const HeavyArgs& a, int threads, int num_sms,
+                             cudaStream_t s);
+size_t heavy_win_smem_bytes(int threads, int vcap, int wcap_bits);
 
 // Windowed numeric phase of heavy rows (k_heavy_w32.cu): a warp per row walks
 // the row's column blocks in windows of at most `cap` distinct columns.

@@ -303,6 +303,12 @@ class Engine:
                                  _stream_handle(stream)), "autotune")
         return self.get_config()
 
+    def autotune_trials(self) -> dict:
+        """Candidates of the last autotune: timed, and pruned by the descriptors."""
+        t, p = ctypes.c_int32(), ctypes.c_int32()
+        check(lib().spg_autotune_trials(self._h, ctypes.byref(t), ctypes.byref(p)), "trials")
+        return {"timed": t.value, "pruned": p.value}
+
     def transpose(self, A: CsrDevice, stream=None) -> CsrDevice:
         dev = A.rowptr.device
         tp = torch.empty(A.n + 1, dtype=torch.int32, device=dev)

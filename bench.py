@@ -568,6 +568,9 @@ def aggregate_serve(runs):
         if len(runs) > 1:
             out[k + "_range"] = [v[0], v[-1]] if v else None
     out["streams"] = len(runs)
+    splits = [r["small_split"] for r in runs if r.get("small_split")]
+    if splits:  # the time split of small requests, per stream
+        out["small_split"] = splits[0] if len(splits) == 1 else splits
     return out
 
 
@@ -629,6 +632,18 @@ def serve_once(pool, ds, prods, rate, label, kw, picks, tasks, gaps):
 
     def pct(v, q):
         return round(v[min(len(v) - 1, int(q * len(v)))], 3) if v else None
+
+    # where a small request's latency goes: queued until a worker took it,
+    # its symbolic pass, waiting for budget after it, and the numeric run
+    def split(sel):
+        parts = {"queued": ("submit_ms", "start_ms"), "planning": ("start_ms", "planned_ms"),
+                 "admission": ("planned_ms", "run_ms"), "running": ("run_ms", "done_ms")}
+        out = {}
+        for name, (a, b) in parts.items():
+            v = sorted(i[b] - i[a] for k, i in ok
+                       if sel(k) and a in i and b in i and i[b] >= i[a] > 0)
+            out[name + "_p50_ms"] = pct(v, 0.5)
+        return out
     work = sum(2.0 * prods[(int(picks[k]), str(tasks[k]))] for k, _ in ok)
     span_s = (max(i["done_ms"] for _, i in ok) - min(i["submit_ms"] for _, i in ok)) / 1e3 \
         if ok else 0.0
@@ -638,6 +653,7 @@ def serve_once(pool, ds, prods, rate, label, kw, picks, tasks, gaps):
             "p50_ms": pct(lat, 0.5), "p99_ms": pct(lat, 0.99),
             "small_requests": len(small),
             "small_p50_ms": pct(small, 0.5), "small_p99_ms": pct(small, 0.99),
+            "small_split": split(lambda k: pool[int(picks[k])][0].n < 65536),
             "sustained_gflops": round(work / span_s / 1e9, 3) if ok and span_s > 0 else None,
             "peak_reserved_gb": round(st["peak_reserved_bytes"] / 1e9, 2)}
 

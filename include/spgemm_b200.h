@@ -118,7 +118,19 @@ typedef struct spg_config {
                                  retire often and work on a higher-priority
                                  stream can start in between (the server's
                                  large-request workers use this)               */
-  int64_t reserved[3];
+  int64_t small_max_nnz;      /* A·A and A·Aᵀ of matrices with at most this many
+                                 entries (and n <= 65,536) are planned with one
+                                 host synchronisation (every row in one launch
+                                 per phase); a row of more than 1536 products
+                                 sends the plan to the regular path; 0 → 2^20,
+                                 negative → never                               */
+  int64_t heavy_vcap;         /* heavy CTA rows: values held in shared memory per
+                                 column window (1024..16384, a power of two),
+                                 each window's values written to C once; 0 →
+                                 8192 (16384 with 1024-thread CTAs); negative →
+                                 accumulate in place in C (the dense-window
+                                 kernel, also taken without block counts)       */
+  int64_t reserved[1];
 } spg_config;
 
 /* Result record of spg_run_ours: the reference's EngResult {ms, nnz, s, as, sq}
@@ -183,7 +195,9 @@ spg_status spg_check_device_status(spg_ctx* ctx, void* stream);
 
 /* ---- plan / execute (replaces the sizing half of run_ours) ---------------- */
 /* Pre-pass + binning + symbolic phase.  Three host synchronisations, each a
- * small pinned readback: the validity verdict on A, the bin sizes, nnz(C).
+ * small pinned readback: the validity verdict on A, the bin sizes, nnz(C);
+ * one (verdict, nnz(C) and row statistics together) for the small matrices
+ * of spg_config.small_max_nnz.
  * When it returns, no kernel of the plan's symbolic phase is still running.
  * A must stay valid until the plan is destroyed. */
 spg_status spg_plan_create(spg_ctx* ctx, spg_task task, const spg_csr_dev* A,
@@ -235,6 +249,11 @@ spg_status spg_get_config(const spg_ctx* ctx, spg_config* cfg);
  * copies it to *best.  Costs a few dozen products of A. */
 spg_status spg_autotune(spg_ctx* ctx, spg_task task, int32_t count, const spg_csr_dev* As,
                         int32_t reps, spg_config* best, void* stream);
+/* Candidates of the last spg_autotune on ctx: `timed` configurations run
+ * (the start included), `pruned` left out because A's structural features
+ * (spg_describe: mean degree, largest row and column degree; the features the
+ * reference's dispatcher reads, bench/dispatch.cu:26-38) rule them out. */
+spg_status spg_autotune_trials(const spg_ctx* ctx, int32_t* timed, int32_t* pruned);
 
 /* ---- serving ---------------------------------------------------------------
  * A request loop for A·A / A·Aᵀ requests of different sizes.  Worker threads,

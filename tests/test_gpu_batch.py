@@ -133,6 +133,11 @@ def test_autotune_keeps_results_exact(eng):
         cfg = e.autotune(dev(A), "AA", reps=1)
         assert cfg["num_load_pct"] in (40, 50, 66, 80)
         assert cfg["lanes_per_row"] in (0, 4, 8, 16, 32)
+        # the descriptors leave out lanes far from the mean degree (12: 16 and
+        # its neighbours stay) and the table cap (rows need at most ~2048 slots
+        # only if their products say so)
+        tr = e.autotune_trials()
+        assert tr["timed"] >= 1 and tr["pruned"] >= 1
         C = e.multiply(dev(A), "AA")
         torch.cuda.synchronize()
         rp, ci, cx = C.to_host()

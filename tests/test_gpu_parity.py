@@ -24,10 +24,13 @@ torch = pytest.importorskip("torch")
 TASKS = ("AA", "AAt", "AAtS")
 
 
-@pytest.fixture(scope="module")
-def eng():
+# Every engine test runs twice: with the default configuration (A·A and A·Aᵀ
+# of matrices up to 2^20 entries take the one-readback plan: one warp-per-row
+# launch per phase) and with that plan switched off (the binned kernels).
+@pytest.fixture(scope="module", params=["default", "binned"])
+def eng(request):
     from appt_spgemm_b200.engine import Engine
-    e = Engine("cuda:0")
+    e = Engine("cuda:0", **({} if request.param == "default" else {"small_max_nnz": -1}))
     yield e
     e.check_device_status()
     e.close()
@@ -80,7 +83,7 @@ def test_wide_rows_three_digit_passes(eng, deg, task):
 @pytest.mark.parametrize("lanes", [4, 8, 16, 32])
 def test_lanes_per_row(lanes):
     from appt_spgemm_b200.engine import Engine
-    with Engine("cuda:0", lanes_per_row=lanes) as e:
+    with Engine("cuda:0", lanes_per_row=lanes, small_max_nnz=-1) as e:
         for task in TASKS:
             run_case(e, csr.erdos_renyi(3000, 9.0, seed=lanes), task, f"er/lanes{lanes}")
 
@@ -100,6 +103,26 @@ def test_force_heavy_dense_windows(window, split):
                        (csr.erdos_renyi(20000, 4.0, seed=3), "er20k")):
             for task in TASKS:
                 run_case(e, A, task, f"forced/{lab}/w{window}")
+
+
+@pytest.mark.parametrize("vcap", [1024, 8192, -1])
+def test_heavy_shared_value_windows(vcap):
+    """Heavy CTA rows with their values in shared memory window by window:
+    1024 values per window (many windows per row; blocks above it cut into
+    fixed 1024-column sub-windows), the default 8192, and -1 (the kernel that
+    accumulates in place in C); every row forced heavy and onto the CTA kernel,
+    then R-MAT heavy rows and 32768-column blocks under the default rules."""
+    from appt_spgemm_b200.engine import Engine
+    with Engine("cuda:0", force_heavy=1, heavy_split=1, heavy_vcap=vcap) as e:
+        for A, lab in ((csr.laplace2d(40), "lap40"), (csr.rmat(11, 8, seed=2), "rmat11"),
+                       (csr.erdos_renyi(20000, 4.0, seed=3), "er20k")):
+            for task in TASKS:
+                run_case(e, A, task, f"win{vcap}/{lab}")
+    with Engine("cuda:0", heavy_vcap=vcap) as e:
+        for task in TASKS:
+            run_case(e, csr.rmat(13, 16, seed=3), task, f"win{vcap}/rmat13")
+    with Engine("cuda:0", heavy_vcap=vcap, heavy_block_budget=1 << 16) as e:
+        run_case(e, csr.erdos_renyi(30000, 90.0, seed=6), "AA", f"win{vcap}/er30k")
 
 
 @pytest.mark.parametrize("task", TASKS)
@@ -129,6 +152,29 @@ def test_rmat_heavy_split(split, task):
     from appt_spgemm_b200.engine import Engine
     with Engine("cuda:0", heavy_split=split) as e:
         run_case(e, csr.rmat(14, 16, seed=4), task, f"rmat14/split{split}")
+
+
+def test_one_readback_plan(eng):
+    """Small A·A and A·Aᵀ plans: with the default configuration one launch per
+    phase (a single bin), and a matrix with a row of more than 1536 products
+    planned again on the binned path — both bit-exact."""
+    A = csr.laplace2d(64)
+    default = eng.get_config()["small_max_nnz"] > 0
+    for task in ("AA", "AAt"):
+        p = eng.plan(dev(A), task)
+        if default:
+            assert p.info["bins_used"] == 1 and p.info["heavy_rows"] == 0
+        p.close()
+        run_case(eng, A, task, "small/laplace64")
+    # one dense row: 1,999 products in row 0
+    n = 3000
+    rows = [np.arange(n, dtype=np.int32)] + [np.array([i], np.int32) for i in range(1, n)]
+    rows[0] = np.arange(0, n, 3, dtype=np.int32)
+    rp = np.concatenate([[0], np.cumsum([len(r) for r in rows])]).astype(np.int32)
+    B = csr.CsrHost(n, rp, np.concatenate(rows),
+                    np.random.default_rng(5).uniform(-1, 1, int(rp[-1])))
+    for task in TASKS:
+        run_case(eng, B, task, "small/fallback")
 
 
 @pytest.mark.parametrize("task", TASKS)
