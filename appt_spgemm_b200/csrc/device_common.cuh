@@ -65,7 +65,10 @@ __device__ __forceinline__ int hash_insert(int* keys, int j, uint32_t* status) {
 // CAS-first linear probe of the warp kernels: one shared atomic per probe, the
 // loop exits on an empty slot (claimed) or on the key itself (reading the slot
 // first and claiming only empty ones measured slower: 3.32 vs 2.88 ms for the
-// numeric phase of the 96³ stencil).  In the numeric phase the value is then
+// numeric phase of the 96³ stencil; so did claims without atomics — a round of
+// read, __match_any_sync grouping of the lanes that saw an empty slot, write by
+// each group's lowest lane and two __syncwarp per round — 4.48 vs 2.83 ms per
+// numeric launch and 2.25 vs 1.07 ms per symbolic one).  In the numeric phase the value is then
 // 0.0 + v for a freshly claimed slot and slot + v otherwise, so no value array
 // is cleared between rows.
 template <int LOG2T, bool NUMERIC>
@@ -88,54 +91,6 @@ __device__ __forceinline__ void insert_acc(int* keys, double* vals, int j, doubl
     double cur = 0.0;
     if (old != kEmptyKey) cur = vals[h];
     vals[h] = __dadd_rn(cur, v);
-  }
-}
-
-// Insert of one segment by a whole warp that owns the table (every lane
-// calls; lanes without a key pass j < 0).  Slots are claimed without shared
-// atomics: in each round every pending lane reads its slot; the lanes that see
-// an empty slot are grouped by slot (__match_any_sync) and the lowest lane of
-// each group writes its key there; lanes that see their own key are done;
-// lanes that see another key move to the next slot; the other lanes of a group
-// read the same slot again in the next round (it may now hold their key).  No
-// other warp touches the table, so a __syncwarp between a round's reads and its
-// writes and one after the writes order every access.  NUMERIC: a claimed
-// slot's value becomes 0.0 + v and a found slot's value slot + v (the keys of
-// one call are distinct, so no two lanes write one value; the closing
-// __syncwarp keeps the k order between calls).  A table that stays full for
-// 2T + 2 rounds is reported, never spun on.
-template <int LOG2T, bool NUMERIC>
-__device__ __forceinline__ void warp_insert(int* keys, double* vals, int j, double v,
-                                            uint32_t* status) {
-  constexpr unsigned T = 1u << LOG2T;
-  const unsigned lane_bit = 1u << (threadIdx.x & 31);
-  unsigned h = hash_slot<LOG2T>(j);
-  bool pending = j >= 0;
-#pragma unroll 1
-  for (unsigned round = 0; __any_sync(0xffffffffu, pending); ++round) {
-    if (round > 2 * T + 1) {
-      if (pending) report(status, DEV_ERR_HASH_FULL);
-      break;
-    }
-    const int cur = pending ? keys[h] : 0;
-    const bool found = pending && cur == j;
-    const bool empty = pending && cur == kEmptyKey;
-    const unsigned em = __ballot_sync(0xffffffffu, empty);
-    bool win = false;
-    if (empty) {
-      const unsigned grp = __match_any_sync(em, h);
-      win = (grp & (0u - grp)) == lane_bit;
-    }
-    __syncwarp();
-    if (win) {
-      keys[h] = j;
-      if (NUMERIC) vals[h] = __dadd_rn(0.0, v);
-    } else if (NUMERIC && found) {
-      vals[h] = __dadd_rn(vals[h], v);
-    }
-    if (win || found) pending = false;
-    else if (pending && !empty) h = (h + 1) & (T - 1);
-    __syncwarp();
   }
 }
 

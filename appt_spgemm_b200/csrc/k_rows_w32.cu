@@ -29,12 +29,6 @@ namespace spg {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
-#ifndef SPG_W32_CAS
-#define SPG_W32_CAS 0
-#endif
-// 1: the CAS-first probe (insert_acc) per lane; 0: warp_insert's atomic-free
-// claims.
-constexpr bool kCasInsert = SPG_W32_CAS != 0;
 // Rows of more entries than this sort with the radix sort rather than the
 // register bitonic network (whose 8-per-lane form costs about 1,000 warp
 // instructions a row against about 600 for two or three digit passes).
@@ -197,14 +191,10 @@ __global__ void __launch_bounds__(256, 5) k_hash_w32(RowArgs a) {
 #pragma unroll
           for (int d = 0; d < D; ++d) {
             const int j = jr[d];
-            const bool use = j >= 0 && !(NUMERIC && GRAM && j < row);
-            const double p = NUMERIC ? __dmul_rn(ar[d], br[d]) : 0.0;
-            if (kCasInsert) {
-              if (use) insert_acc<LOG2T, NUMERIC>(keys, vals, j, p, a.status);
-              if (NUMERIC) __syncwarp();  // k-order of the accumulation
-            } else {
-              warp_insert<LOG2T, NUMERIC>(keys, vals, use ? j : -1, p, a.status);
-            }
+            if (j >= 0 && !(NUMERIC && GRAM && j < row))
+              insert_acc<LOG2T, NUMERIC>(keys, vals, j, NUMERIC ? __dmul_rn(ar[d], br[d]) : 0.0,
+                                         a.status);
+            if (NUMERIC) __syncwarp();  // k-order of the accumulation
           }
         }
         continue;
@@ -250,14 +240,10 @@ __global__ void __launch_bounds__(256, 5) k_hash_w32(RowArgs a) {
 #pragma unroll
         for (int d = 0; d < D; ++d) {
           const int j = jr[d];
-          const bool use = j >= 0 && !(NUMERIC && GRAM && j < row);
-          const double p = NUMERIC ? __dmul_rn(ar[d], br[d]) : 0.0;
-          if (kCasInsert) {
-            if (use) insert_acc<LOG2T, NUMERIC>(keys, vals, j, p, a.status);
-            if (NUMERIC) __syncwarp();  // k-order of the accumulation
-          } else {
-            warp_insert<LOG2T, NUMERIC>(keys, vals, use ? j : -1, p, a.status);
-          }
+          if (j >= 0 && !(NUMERIC && GRAM && j < row))
+            insert_acc<LOG2T, NUMERIC>(keys, vals, j, NUMERIC ? __dmul_rn(ar[d], br[d]) : 0.0,
+                                       a.status);
+          if (NUMERIC) __syncwarp();  // k-order of the accumulation
         }
       }
     }

@@ -182,9 +182,10 @@ bool plan_job(spg_server* s, spg_ctx* ctx, cudaStream_t st, Job& j, std::vector<
   }
   spg_plan_get_info(j.p, &j.info);
   const size_t b = j.rs.size();
-  j.row_off.resize(b + 1);
-  j.nnz_off.resize(b + 1);
-  j.out_r.resize(b);
+  j.row_off.assign(b + 1, 0);
+  j.nnz_off.assign(b + 1, 0);
+  j.out_r.assign(b, 0);
+  j.outs = 0;  // a batch planned again after waiting counts its outputs afresh
   spg_plan_batch_offsets(j.p, j.row_off.data(), j.nnz_off.data());
   for (size_t i = 0; i < b; ++i) {
     j.out_r[i] = output_bytes(j.rs[i]->A.n, j.nnz_off[i + 1] - j.nnz_off[i]);

@@ -234,6 +234,18 @@ def test_invalid_csr_rejected_on_device(eng):
             with pytest.raises(SpgemmError) as e:
                 eng.multiply(M, task)
             assert e.value.status == _capi.SPG_ERR_INVALID_CSR
+    # row pointers out of range and decreasing (the one-readback plan runs its
+    # kernels before it sees the verdict: they must stay inside the arrays)
+    far, swapped = A.rowptr.copy(), A.rowptr.copy()
+    far[3] = 10**6
+    swapped[5], swapped[6] = swapped[6], swapped[5]
+    for rp in (far, swapped):
+        M = CsrDevice(A.n, torch.from_numpy(rp).cuda(), torch.from_numpy(A.col).cuda(),
+                      torch.from_numpy(A.val).cuda())
+        for task in TASKS:
+            with pytest.raises(SpgemmError) as e:
+                eng.multiply(M, task)
+            assert e.value.status == _capi.SPG_ERR_INVALID_CSR
     with pytest.raises(SpgemmError):
         eng.multiply(dev(A), "AB")
 

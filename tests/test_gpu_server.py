@@ -2,6 +2,8 @@
 oracle) bit for bit while requests of different sizes run concurrently and
 small ones are merged into batches; the memory budget rejects what can never
 fit and holds back what does not fit yet."""
+import time
+
 import numpy as np
 import pytest
 
@@ -203,12 +205,24 @@ def test_server_holds_at_most_its_budget():
     budget = int(max(need, bound) * 2.5)
     with Server(workers=3, memory_budget_bytes=budget, batch_rows=1) as srv:
         ids = [srv.submit(d, "AA") for _ in range(6)]
-        for rid in ids:
-            assert srv.wait(rid, 120000)["status"] == _capi.SPG_OK
-            got = srv.result(rid).to_host()
-            for x, y in zip(got, alone):
-                assert np.array_equal(x.view(np.uint8), y.view(np.uint8))
-            srv.release(rid)
+        # results are checked and released as they complete: the workers may
+        # finish requests out of submission order, and a client that kept later
+        # results while waiting for an earlier one could hold the budget that
+        # the earlier one needs
+        pending, deadline = set(ids), time.time() + 120
+        while pending:
+            assert time.time() < deadline, f"requests {sorted(pending)} did not complete"
+            for rid in sorted(pending):
+                info = srv.poll(rid)
+                if info["status"] == _capi.SPG_ERR_NOT_READY:
+                    continue
+                assert info["status"] == _capi.SPG_OK
+                got = srv.result(rid).to_host()
+                for x, y in zip(got, alone):
+                    assert np.array_equal(x.view(np.uint8), y.view(np.uint8))
+                srv.release(rid)
+                pending.discard(rid)
+            time.sleep(0.001)
         st = srv.stats()
         assert st["completed"] == 6 and st["rejected"] == 0
         assert 0 < st["peak_held_bytes"] <= budget
