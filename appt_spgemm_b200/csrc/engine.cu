@@ -236,6 +236,9 @@ spg_config merged_config(const spg_config* user) {
   if (c.grid_sms < 0) c.grid_sms = 0;
   if (c.grid_sms > (1 << 16)) c.grid_sms = 1 << 16;
   if (c.small_max_nnz == 0) c.small_max_nnz = kSmallMaxNnzDefault;
+  if (c.dense_max_words == 0) c.dense_max_words = (int64_t)1 << kDenseMaxLog2W;
+  if (c.dense_max_words > ((int64_t)1 << kDenseMaxLog2W))
+    c.dense_max_words = (int64_t)1 << kDenseMaxLog2W;
   if (c.heavy_vcap > 0) {  // a power of two in [1024, 16384]
     int64_t v = 1024;
     while (v * 2 <= c.heavy_vcap && v < 16384) v *= 2;
@@ -622,11 +625,18 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
   const int64_t split = ctx->cfg.heavy_split > 0 ? (int64_t)ctx->cfg.heavy_split
                                                  : kHeavySplitDefault;
   const int short_lg = std::min(num_lg, 11);
+  // bitmap bins (not for the Gram path): the largest bitmap the config allows
+  int dense_lw = -1;
+  if (!gram && ctx->cfg.dense_max_words >= (1 << kDenseMinLog2W)) {
+    dense_lw = kDenseMinLog2W;
+    while (dense_lw < kDenseMaxLog2W && ((int64_t)2 << dense_lw) <= ctx->cfg.dense_max_words)
+      ++dense_lw;
+  }
   BinSource bsym{0, n, p->f, p->lo, p->hi, nullptr, nullptr, kMaxTableLog2, force,
                  ctx->cfg.sym_load_pct,
                  numeric_heavy_min(num_lg, ctx->cfg.num_load_pct),
                  p->A.rowptr, split, short_lg,
-                 numeric_heavy_min(short_lg, ctx->cfg.num_load_pct)};
+                 numeric_heavy_min(short_lg, ctx->cfg.num_load_pct), dense_lw};
   {
     ProfScope ps(ctx, "plan/bin_sym", st);
     TRY_CUDA(launch_bin_rows(bsym, hist, counts, rows_sym, st), "symbolic binning");
@@ -701,6 +711,15 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
     ProfScope ps(ctx, "sym/bin", st, b);
     TRY_CUDA(launch_hash_bin(b, false, gram, r, ctx->num_sms, st), "symbolic");
   }
+  for (int b = kDenseBin0; b < kNumBins; ++b) {
+    if (sym_count[b] == 0) continue;
+    ++bins_used;
+    RowArgs r = ra;
+    r.rows = rows_sym + sym_start[b];
+    r.nrows = (int32_t)sym_count[b];
+    ProfScope ps(ctx, "sym/dense", st, b - kDenseBin0 + kDenseMinLog2W);
+    TRY_CUDA(launch_dense_bin(b, false, r, ctx->num_sms, st), "symbolic");
+  }
   if (sym_count[kHeavyBin] > 0) {
     HeavyArgs h{};
     h.r = ra;
@@ -736,7 +755,7 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
   // numeric binning by exact counts, stats; host sync #3 (nnz(C))
   TRY(palloc(p, &p->rows_num, n));
   BinSource bnum{1, n, p->f, p->lo, p->hi, p->rownnz, gram ? p->rowlow : nullptr, num_lg, force,
-                 ctx->cfg.num_load_pct, 0, p->A.rowptr, split, short_lg, 0};
+                 ctx->cfg.num_load_pct, 0, p->A.rowptr, split, short_lg, 0, dense_lw};
   {
     ProfScope ps(ctx, "plan/bin_num", st);
     TRY_CUDA(launch_bin_rows(bnum, hist, counts + 2 * kNumBins, p->rows_num, st),
@@ -868,6 +887,15 @@ spg_status execute_impl(spg_plan* p, spg_csr_out* C, cudaStream_t st) {
       r.G = hash_bin_lanes(b, p->G);
       ProfScope ps(ctx, "num/bin", st, b);
       cudaError_t e = launch_hash_bin(b, true, gram, r, ctx->num_sms, st);
+      if (e != cudaSuccess) result = cuda_status(e, "numeric");
+    }
+    for (int b = kDenseBin0; b < kNumBins && result == SPG_OK; ++b) {
+      if (p->num_count[b] == 0) continue;
+      RowArgs r = ra;
+      r.rows = p->rows_num + p->num_start[b];
+      r.nrows = (int32_t)p->num_count[b];
+      ProfScope ps(ctx, "num/dense", st, b - kDenseBin0 + kDenseMinLog2W);
+      cudaError_t e = launch_dense_bin(b, true, r, ctx->num_sms, st);
       if (e != cudaSuccess) result = cuda_status(e, "numeric");
     }
     if (result != SPG_OK) break;

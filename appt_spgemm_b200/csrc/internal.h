@@ -30,9 +30,14 @@ constexpr int kMinTableLog2 = 4;       // smallest shared table: 16 slots
 constexpr int kMaxTableLog2 = 14;      // largest shared table: 16384 slots
 constexpr int kNumTableBins = kMaxTableLog2 - kMinTableLog2 + 1;  // 11
 // Row bins: 0 = empty row, 1..kNumTableBins = shared table of 2^(bin+3) slots,
-// kHeavyBin = heavy row (CTA per row, dense column window).
+// kHeavyBin = heavy row (CTA per row, dense column window), kDenseBin0 + b =
+// warp row over a bitmap of 2^(kDenseMinLog2W + b) words of its column span.
 constexpr int kEmptyBin = 0;
 constexpr int kHeavyBin = kNumTableBins + 1;  // 12
-constexpr int kNumBins = kHeavyBin + 1;       // 13
+constexpr int kDenseMinLog2W = 8;
+constexpr int kDenseMaxLog2W = 11;
+constexpr int kDenseBin0 = kHeavyBin + 1;     // 13
+constexpr int kNumBins = kDenseBin0 + kDenseMaxLog2W - kDenseMinLog2W + 1;  // 17
+constexpr int kDenseVals = 512;  // entries of a bitmap-path row (numeric)
 
 }  // namespace spg

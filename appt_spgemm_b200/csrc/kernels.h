@@ -52,6 +52,11 @@ struct BinSource {
   int64_t short_split;
   int short_max_log2;
   int64_t short_min;
+  // rows whose output span fits 2^dense_max_log2w bitmap words, at most twice
+  // their products, with at least 64 products (and, numeric, at most
+  // kDenseVals entries) take the bitmap bins; dense_max_log2w < kDenseMinLog2W:
+  // never (the Gram path, or switched off)
+  int dense_max_log2w;
 };
 
 __host__ __device__ __forceinline__ int ceil_log2_64(int64_t x) {
@@ -79,6 +84,18 @@ __host__ __device__ __forceinline__ int row_bin(const BinSource& s, int i) {
   const int64_t want = size * 100 / s.load_pct + 1;
   if (s.force_heavy) return kHeavyBin;
   if (s.mode == 0 && s.heavy_min > 0 && size >= s.heavy_min) return kHeavyBin;
+  if (s.dense_max_log2w >= kDenseMinLog2W) {
+    const int64_t words = ((int64_t)s.hi[i] - s.lo[i] + 32) >> 5;
+    const int64_t f = s.f[i];
+    // (symbolic: only rows the numeric binning can never send heavy, which
+    // need the heavy symbolic kernel's block counts)
+    if (f >= 64 && words <= 2 * f && words <= ((int64_t)1 << s.dense_max_log2w) &&
+        (s.mode == 0 ? (s.short_split <= 0 || size < s.short_min) : size <= kDenseVals)) {
+      int lw = ceil_log2_64(words);
+      if (lw < kDenseMinLog2W) lw = kDenseMinLog2W;
+      return kDenseBin0 + lw - kDenseMinLog2W;
+    }
+  }
   int lg = ceil_log2_64(want);
   if (lg < kMinTableLog2) lg = kMinTableLog2;
   if (lg > s.max_log2) return kHeavyBin;
@@ -198,6 +215,9 @@ cudaError_t launch_hash_w32(int log2t, bool numeric, bool gram, const RowArgs& a
 // upper part only plus the mirror append).
 cudaError_t launch_hash_bin(int bin, bool numeric, bool gram, const RowArgs& a, int num_sms,
                             cudaStream_t s);
+// Warp-per-row bitmap kernels of the dense bins (k_dense_w32.cu; not Gram).
+cudaError_t launch_dense_bin(int bin, bool numeric, const RowArgs& a, int num_sms,
+                             cudaStream_t s);
 int hash_bin_lanes(int bin, int lanes_cfg);
 
 // ---- heavy rows: dense column windows (k_heavy.cu) --------------------------

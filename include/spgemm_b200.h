@@ -130,7 +130,10 @@ typedef struct spg_config {
                                  8192 (16384 with 1024-thread CTAs); negative →
                                  accumulate in place in C (the dense-window
                                  kernel, also taken without block counts)       */
-  int64_t reserved[1];
+  int64_t dense_max_words;    /* rows whose output column span fits this many
+                                 32-bit bitmap words (256..2048) and is at most
+                                 twice their products take the bitmap kernels
+                                 (A·A, A·Aᵀ); 0 → 2048; negative → never        */
 } spg_config;
 
 /* Result record of spg_run_ours: the reference's EngResult {ms, nnz, s, as, sq}

@@ -177,6 +177,26 @@ def test_one_readback_plan(eng):
         run_case(eng, B, task, "small/fallback")
 
 
+@pytest.mark.parametrize("words", [256, 512, 1024, -1])
+def test_dense_bitmap_rows(words):
+    """Rows over a bitmap of their output span (bitmap bins of up to 256, 512
+    and 1024 words, or switched off): stencils, banded matrices and a random
+    graph (whose spans are too wide, so it stays on the hash tables), all
+    tasks (the Gram path never takes the bitmap bins)."""
+    from appt_spgemm_b200.engine import Engine
+    cases = [(csr.stencil27(12, 5), "st12"), (csr.stencil27(30, 6), "st30"),
+             (csr.banded(3000, 30, 0.3, 7), "band30"), (csr.banded(20000, 64, 0.3, 8), "band64"),
+             (csr.uniform(4000, 40, seed=9), "uni40"), (csr.laplace2d(50), "lap50")]
+    with Engine("cuda:0", small_max_nnz=-1, dense_max_words=words) as e:
+        for A, lab in cases:
+            for task in TASKS:
+                run_case(e, A, task, f"dense{words}/{lab}")
+        # spans of 458 and 521 words: the 512- and 1024-word bins
+        for A, lab in ((csr.stencil27(60, 11), "st60"), (csr.stencil27(64, 12), "st64")):
+            run_case(e, A, "AA", f"dense{words}/{lab}")
+        e.check_device_status()
+
+
 @pytest.mark.parametrize("task", TASKS)
 def test_stencil27_small(eng, task):
     run_case(eng, csr.stencil27(18, seed=2), task, "stencil27_18")
