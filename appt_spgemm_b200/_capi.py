@@ -55,7 +55,7 @@ class SpgConfig(Structure):
                 ("num_load_pct", c_int32), ("heavy_split", c_int32),
                 ("pool_release_bytes", c_int64), ("heavy_block_budget", c_int64),
                 ("grid_sms", c_int64), ("small_max_nnz", c_int64), ("heavy_vcap", c_int64),
-                ("dense_max_words", c_int64)]
+                ("dense_max_words", c_int64), ("bin_streams", c_int32), ("pad0", c_int32)]
 
 
 class SpgEngResult(Structure):

@@ -45,6 +45,12 @@ struct spg_ctx {
   std::vector<ProfEntry> pending;
   std::map<std::string, std::pair<double, long long>> prof_acc;
   int32_t tune_timed = 0, tune_pruned = 0;  // the last spg_autotune's candidates
+  // concurrent bin launches: side streams forked from the caller's stream
+  static constexpr int kMaxSides = 8;
+  cudaStream_t side[kMaxSides] = {};
+  cudaEvent_t side_done[kMaxSides] = {};
+  cudaEvent_t fork_ev = nullptr;
+  int nsides = 0;
   std::vector<cudaEvent_t> event_pool;
   long long launch_base = 0;
 };
@@ -82,6 +88,44 @@ struct ProfScope {
     cudaEventRecord(b, s);
     c->pending.push_back(ProfEntry{label, a, b});
   }
+};
+
+// Launches of different row bins of one phase touch disjoint rows, so they may
+// overlap: each bin gets the next side stream (forked from the caller's stream
+// by an event, so it starts after everything queued there), and join() makes
+// the caller's stream wait for all of them.  With one bin, or bin_streams 1,
+// everything stays on the caller's stream.  Fork and join are events, which a
+// stream capture records as graph edges.
+struct BinFork {
+  spg_ctx* c;
+  cudaStream_t main;
+  int ns;  // side streams in use
+  bool on;
+  int used = 0;
+  BinFork(spg_ctx* ctx, cudaStream_t st, int launches)
+      : c(ctx), main(st), ns(std::min(ctx->nsides, (int)ctx->cfg.bin_streams)),
+        on(launches > 1 && ns > 1) {
+    if (on && cudaEventRecord(c->fork_ev, main) != cudaSuccess) on = false;
+  }
+  cudaStream_t next() {
+    if (!on) return main;
+    const int i = used % ns;
+    if (used < ns) cudaStreamWaitEvent(c->side[i], c->fork_ev, 0);
+    ++used;
+    return c->side[i];
+  }
+  cudaError_t join() {
+    if (!on) return cudaSuccess;
+    const int k = used < ns ? used : ns;
+    for (int i = 0; i < k; ++i) {
+      cudaError_t e = cudaEventRecord(c->side_done[i], c->side[i]);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(main, c->side_done[i], 0);
+      if (e != cudaSuccess) return e;
+    }
+    on = false;
+    return cudaSuccess;
+  }
+  ~BinFork() { join(); }
 };
 
 void prof_resolve(spg_ctx* c) {
@@ -149,7 +193,8 @@ struct spg_plan {
   // numeric one with tables of 2^small_log2 slots
   bool small = false;
   int small_log2 = 6;
-  int32_t* hqueue = nullptr;  // next row of the CTA-per-row kernels (zeroed before each launch)
+  int32_t* hqueue = nullptr;  // next row of the CTA-per-row kernels, one counter per bin
+                              // (zeroed before each launch; bins may run at once)
   int window_bits = 1 << 20;  // heavy-path shape (heavy_shape)
   int heavy_threads = 1024;
 };
@@ -237,6 +282,8 @@ spg_config merged_config(const spg_config* user) {
   if (c.grid_sms > (1 << 16)) c.grid_sms = 1 << 16;
   if (c.small_max_nnz == 0) c.small_max_nnz = kSmallMaxNnzDefault;
   if (c.dense_max_words == 0) c.dense_max_words = (int64_t)1 << kDenseMaxLog2W;
+  if (c.bin_streams <= 0) c.bin_streams = 4;
+  if (c.bin_streams > spg_ctx::kMaxSides) c.bin_streams = spg_ctx::kMaxSides;
   if (c.dense_max_words > ((int64_t)1 << kDenseMaxLog2W))
     c.dense_max_words = (int64_t)1 << kDenseMaxLog2W;
   if (c.heavy_vcap > 0) {  // a power of two in [1024, 16384]
@@ -428,7 +475,7 @@ spg_status plan_build_small(spg_plan* p, const spg_csr_dev* Ad, bool* fallback) 
   const size_t nn = (size_t)(n > 0 ? n : 1), nz = (size_t)(nnz > 0 ? nnz : 1);
   const size_t o_f = take(8 * nn), o_lo = take(4 * nn), o_hi = take(4 * nn),
                o_cnt = take(4 * nn), o_rp = take(8 * (nn + 1)), o_scan = take(scan_tmp_bytes(n)),
-               o_stats = take(32), o_q = take(4);
+               o_stats = take(32), o_q = take(4 * kNumBins);
   size_t o_bp = 0, o_bi = 0, o_bx = 0, o_tc = 0, o_tu = 0, o_ts = 0, o_tk = 0, o_tv = 0,
          o_ll = 0, o_lc = 0;
   if (aat) {
@@ -606,7 +653,7 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
   TRY(palloc(p, &p->f, n));
   TRY(palloc(p, &p->lo, n));
   TRY(palloc(p, &p->hi, n));
-  TRY(palloc(p, &p->hqueue, 1));
+  TRY(palloc(p, &p->hqueue, kNumBins));
   {
     ProfScope ps(ctx, "plan/prepass", st);
     TRY_CUDA(launch_prepass(p->A, p->B, p->f, p->lo, p->hi, st), "prepass");
@@ -701,24 +748,28 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
   ra.lo = p->lo;
   ra.hi = p->hi;
   int bins_used = 0;
+  for (int b = 1; b < kNumBins; ++b)
+    if (sym_count[b] > 0) ++bins_used;
+  BinFork fork(ctx, st, bins_used);
   for (int b = 1; b <= kNumTableBins; ++b) {
     if (sym_count[b] == 0) continue;
-    ++bins_used;
     RowArgs r = ra;
     r.rows = rows_sym + sym_start[b];
     r.nrows = (int32_t)sym_count[b];
     r.G = hash_bin_lanes(b, p->G);
-    ProfScope ps(ctx, "sym/bin", st, b);
-    TRY_CUDA(launch_hash_bin(b, false, gram, r, ctx->num_sms, st), "symbolic");
+    r.queue = p->hqueue + b;
+    const cudaStream_t bs = fork.next();
+    ProfScope ps(ctx, "sym/bin", bs, b);
+    TRY_CUDA(launch_hash_bin(b, false, gram, r, ctx->num_sms, bs), "symbolic");
   }
   for (int b = kDenseBin0; b < kNumBins; ++b) {
     if (sym_count[b] == 0) continue;
-    ++bins_used;
     RowArgs r = ra;
     r.rows = rows_sym + sym_start[b];
     r.nrows = (int32_t)sym_count[b];
-    ProfScope ps(ctx, "sym/dense", st, b - kDenseBin0 + kDenseMinLog2W);
-    TRY_CUDA(launch_dense_bin(b, false, r, ctx->num_sms, st), "symbolic");
+    const cudaStream_t bs = fork.next();
+    ProfScope ps(ctx, "sym/dense", bs, b - kDenseBin0 + kDenseMinLog2W);
+    TRY_CUDA(launch_dense_bin(b, false, r, ctx->num_sms, bs), "symbolic");
   }
   if (sym_count[kHeavyBin] > 0) {
     HeavyArgs h{};
@@ -731,11 +782,13 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
     h.blk_off = p->blk_off;
     h.blk_cnt = p->blk_cnt;
     h.blk_log2 = p->blk_log2;
-    h.queue = p->hqueue;
-    ProfScope ps(ctx, "sym/heavy", st);
-    TRY_CUDA(launch_heavy(false, gram, h, p->heavy_threads, ctx->num_sms, st),
+    h.queue = p->hqueue + kHeavyBin;
+    const cudaStream_t bs = fork.next();
+    ProfScope ps(ctx, "sym/heavy", bs);
+    TRY_CUDA(launch_heavy(false, gram, h, p->heavy_threads, ctx->num_sms, bs),
              "symbolic heavy");
   }
+  TRY_CUDA(fork.join(), "join");
 
   // C row pointers (and lower-part offsets of the Gram mirror)
   void* scan_tmp;
@@ -870,6 +923,18 @@ spg_status execute_impl(spg_plan* p, spg_csr_out* C, cudaStream_t st) {
       ra.lcol = (int32_t*)lc;
       ra.lval = (double*)lv;
     }
+    // the heavy rows' cursors are taken from the pool before the bins fork, so
+    // their allocation is ordered before every stream that uses them
+    int4* hcur = nullptr;
+    if (p->num_count[kHeavyBin] > 0 && p->heavy_windows) {  // one int4 per entry of A
+      void* hc;
+      if ((result = talloc(&hc, sizeof(int4) * (size_t)p->A.nnz)) != SPG_OK) break;
+      hcur = (int4*)hc;
+    }
+    int launches = p->small && n > 0 ? 1 : 0;
+    for (int b = 1; b < kNumBins; ++b)
+      if (p->num_count[b] > 0) launches += b == kHeavyBin && p->heavy_windows ? 2 : 1;
+    BinFork fork(ctx, st, launches);
     if (p->small && n > 0) {
       RowArgs r = ra;
       r.rows = nullptr;
@@ -885,8 +950,10 @@ spg_status execute_impl(spg_plan* p, spg_csr_out* C, cudaStream_t st) {
       r.rows = p->rows_num + p->num_start[b];
       r.nrows = (int32_t)p->num_count[b];
       r.G = hash_bin_lanes(b, p->G);
-      ProfScope ps(ctx, "num/bin", st, b);
-      cudaError_t e = launch_hash_bin(b, true, gram, r, ctx->num_sms, st);
+      r.queue = p->hqueue + b;
+      const cudaStream_t bs = fork.next();
+      ProfScope ps(ctx, "num/bin", bs, b);
+      cudaError_t e = launch_hash_bin(b, true, gram, r, ctx->num_sms, bs);
       if (e != cudaSuccess) result = cuda_status(e, "numeric");
     }
     for (int b = kDenseBin0; b < kNumBins && result == SPG_OK; ++b) {
@@ -894,8 +961,9 @@ spg_status execute_impl(spg_plan* p, spg_csr_out* C, cudaStream_t st) {
       RowArgs r = ra;
       r.rows = p->rows_num + p->num_start[b];
       r.nrows = (int32_t)p->num_count[b];
-      ProfScope ps(ctx, "num/dense", st, b - kDenseBin0 + kDenseMinLog2W);
-      cudaError_t e = launch_dense_bin(b, true, r, ctx->num_sms, st);
+      const cudaStream_t bs = fork.next();
+      ProfScope ps(ctx, "num/dense", bs, b - kDenseBin0 + kDenseMinLog2W);
+      cudaError_t e = launch_dense_bin(b, true, r, ctx->num_sms, bs);
       if (e != cudaSuccess) result = cuda_status(e, "numeric");
     }
     if (result != SPG_OK) break;
@@ -913,15 +981,12 @@ spg_status execute_impl(spg_plan* p, spg_csr_out* C, cudaStream_t st) {
       h.cap = heavy_cap(ctx->cfg.num_load_pct);
       h.sub_log2 = 31 - __builtin_clz((unsigned)h.cap);  // largest power of two <= cap
       if (h.sub_log2 > p->blk_log2) h.sub_log2 = p->blk_log2;
-      if (p->heavy_windows) {  // one int4 cursor per entry of A
-        void* hc;
-        if ((result = talloc(&hc, sizeof(int4) * (size_t)p->A.nnz)) != SPG_OK) break;
-        h.hcur = (int4*)hc;
-      }
-      h.queue = p->hqueue;
+      h.hcur = hcur;
+      h.queue = p->hqueue + kHeavyBin;
       // rows fed by many short B rows stream through the warp kernel's
       // windows; rows dominated by long B rows, rows of more than 2^17
-      // products, or all rows without block counts take the CTA kernel
+      // products, or all rows without block counts take the CTA kernel (the
+      // two take disjoint rows, so they run on streams of their own)
       const bool windows = p->heavy_windows;
       h.f = p->f;
       h.split = !windows ? 0
@@ -933,13 +998,23 @@ spg_status execute_impl(spg_plan* p, spg_csr_out* C, cudaStream_t st) {
       h.vcap = ctx->cfg.heavy_vcap > 0 ? (int32_t)ctx->cfg.heavy_vcap
                                        : (win_threads > 512 ? 16384 : 8192);
       h.wcap_bits = win_threads > 512 ? (1 << 18) : (1 << 17);
-      ProfScope ps(ctx, "num/heavy", st);
       cudaError_t e = cudaSuccess;
-      if (windows) e = launch_heavy_w32(gram, h, ctx->num_sms, st);
-      if (e == cudaSuccess)
-        e = shared_values ? launch_heavy_win(gram, h, win_threads, ctx->num_sms, st)
-                          : launch_heavy(true, gram, h, p->heavy_threads, ctx->num_sms, st);
+      if (windows) {
+        const cudaStream_t bs = fork.next();
+        ProfScope ps(ctx, "num/heavy_w32", bs);
+        e = launch_heavy_w32(gram, h, ctx->num_sms, bs);
+      }
+      if (e == cudaSuccess) {
+        const cudaStream_t bs = fork.next();
+        ProfScope ps(ctx, "num/heavy", bs);
+        e = shared_values ? launch_heavy_win(gram, h, win_threads, ctx->num_sms, bs)
+                          : launch_heavy(true, gram, h, p->heavy_threads, ctx->num_sms, bs);
+      }
       if (e != cudaSuccess) { result = cuda_status(e, "numeric heavy"); break; }
+    }
+    {
+      const cudaError_t e = fork.join();
+      if (e != cudaSuccess) { result = cuda_status(e, "join"); break; }
     }
     if (gram && p->nnz_low > 0) {
       void *ll, *lcnt;
@@ -1024,6 +1099,20 @@ spg_status spg_create(spg_ctx** out, const spg_config* cfg) {
     if ((e = cudaMalloc(&ctx->d_status, 256)) != cudaSuccess) { st = cuda_status(e, "status"); break; }
     if ((e = cudaMemset(ctx->d_status, 0, 256)) != cudaSuccess) { st = cuda_status(e, "status"); break; }
     if ((e = cudaMallocHost(&ctx->h_pin, 512)) != cudaSuccess) { st = cuda_status(e, "pinned"); break; }
+    if ((e = cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming)) != cudaSuccess) {
+      st = cuda_status(e, "event");
+      break;
+    }
+    for (int i = 0; i < spg_ctx::kMaxSides && i < ctx->cfg.bin_streams && ctx->cfg.bin_streams > 1;
+         ++i) {
+      if ((e = cudaStreamCreateWithFlags(&ctx->side[i], cudaStreamNonBlocking)) != cudaSuccess ||
+          (e = cudaEventCreateWithFlags(&ctx->side_done[i], cudaEventDisableTiming)) != cudaSuccess) {
+        st = cuda_status(e, "side stream");
+        break;
+      }
+      ctx->nsides = i + 1;
+    }
+    if (st != SPG_OK) break;
   } while (0);
   if (st != SPG_OK) {
     spg_destroy(ctx);
@@ -1042,6 +1131,11 @@ spg_status spg_destroy(spg_ctx* ctx) {
   for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
   if (ctx->d_status) cudaFree(ctx->d_status);
   if (ctx->h_pin) cudaFreeHost(ctx->h_pin);
+  for (int i = 0; i < spg_ctx::kMaxSides; ++i) {
+    if (ctx->side[i]) cudaStreamDestroy(ctx->side[i]);
+    if (ctx->side_done[i]) cudaEventDestroy(ctx->side_done[i]);
+  }
+  if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
   if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
   delete ctx;
   return SPG_OK;

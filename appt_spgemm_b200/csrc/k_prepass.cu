@@ -284,6 +284,29 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_apply(const int32_t* __re
   if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = (OutT)tile_sums[ntiles];
 }
 
+// One tile (n <= kScanTile): the whole scan in one launch.
+template <typename OutT>
+__global__ void __launch_bounds__(kScanThreads) k_scan_single(const int32_t* __restrict__ in,
+                                                              OutT* __restrict__ out, int64_t n) {
+  __shared__ long long scratch[32];
+  const int64_t base = (int64_t)threadIdx.x * kScanItems;
+  int32_t v[kScanItems];
+  long long s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    v[k] = (base + k < n) ? in[base + k] : 0;
+    s += v[k];
+  }
+  long long tot;
+  long long run = block_exclusive_scan64(s, scratch, &tot);
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    if (base + k < n) out[base + k] = (OutT)run;
+    run += v[k];
+  }
+  if (threadIdx.x == 0) out[n] = (OutT)tot;
+}
+
 size_t scan_tmp_bytes(int64_t n) {
   int64_t ntiles = (n + kScanTile - 1) / kScanTile;
   return sizeof(long long) * (size_t)(ntiles + 1);
@@ -294,6 +317,11 @@ static cudaError_t scan_impl(const int32_t* in, OutT* out, int64_t n, void* tmp,
   long long* tile = (long long*)tmp;
   const int64_t ntiles = (n + kScanTile - 1) / kScanTile;
   if (ntiles == 0) return cudaMemsetAsync(out, 0, sizeof(OutT), s);
+  if (ntiles == 1) {
+    k_scan_single<OutT><<<1, kScanThreads, 0, s>>>(in, out, n);
+    SPG_COUNT_LAUNCH();
+    return cudaGetLastError();
+  }
   k_scan_tiles<<<(unsigned)ntiles, kScanThreads, 0, s>>>(in, n, tile);
   SPG_COUNT_LAUNCH();
   k_scan_tile_sums<<<1, 1024, 0, s>>>(tile, ntiles);

@@ -367,6 +367,7 @@ void worker_main(spg_server* s, int index) {
   cfg.device = s->device;
   cfg.pool_release_bytes = 64ll << 20;  // give freed memory back: the budget is global
   if (s->cfg.workers >= 2 && !small_only) cfg.grid_sms = 1 << 16;
+  if (small_only) cfg.bin_streams = 1;  // every launch on the lane's high-priority stream
   spg_ctx* ctx = nullptr;
   const bool ok = spg_create(&ctx, &cfg) == SPG_OK;
   std::deque<Job> waiting;  // admitted to nothing, holding no memory, oldest first

@@ -271,20 +271,23 @@ def cusparse_baseline(dA, A, p_aa, p_aat, reps=5):
     fn.restype = ctypes.c_int
     fn.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                    ctypes.c_longlong, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_float),
-                   ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_longlong),
+                   ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
+                   ctypes.POINTER(ctypes.c_longlong),
                    ctypes.POINTER(ctypes.c_double), ctypes.c_char_p, ctypes.c_int]
     out = {}
     for task, tid, prods in (("AA", 0, p_aa), ("AAt", 1, p_aat)):
-        mean, mn = ctypes.c_float(), ctypes.c_float()
+        mean, mn, med = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
         nnz = ctypes.c_longlong()
         chk = (ctypes.c_double * 3)()
         err = ctypes.create_string_buffer(256)
         rc = fn(tid, dA.rowptr.data_ptr(), dA.col.data_ptr(), dA.val.data_ptr(), A.n, A.nnz, reps, 2,
-                ctypes.byref(mean), ctypes.byref(mn), ctypes.byref(nnz), chk, err, 256)
+                ctypes.byref(mean), ctypes.byref(mn), ctypes.byref(med), ctypes.byref(nnz), chk,
+                err, 256)
         if rc != 0:
             out[task] = {"error": err.value.decode()}
         else:
             out[task] = {"ms_mean": round(mean.value, 4), "ms_min": round(mn.value, 4),
+                         "ms_median": round(med.value, 4),
                          "nnz_c": nnz.value,
                          "gflops": round(2.0 * prods / (mean.value * 1e-3) / 1e9, 3)}
     return out

@@ -134,6 +134,11 @@ typedef struct spg_config {
                                  32-bit bitmap words (256..2048) and is at most
                                  twice their products take the bitmap kernels
                                  (A·A, A·Aᵀ); 0 → 2048; negative → never        */
+  int32_t bin_streams;        /* the kernels of different row bins of one phase
+                                 run concurrently on this many streams (forked
+                                 from and joined back into the caller's
+                                 stream); 0 → 4; 1 → all on the caller's stream */
+  int32_t pad0;
 } spg_config;
 
 /* Result record of spg_run_ours: the reference's EngResult {ms, nnz, s, as, sq}
