@@ -45,9 +45,14 @@ __device__ __forceinline__ int win_rank(const uint32_t* bm, const int* pre4, int
 
 }  // namespace
 
+// Dynamic shared memory, in the order the kernel lays it out: values (vcap
+// doubles), bitmap (wcap/32 words), group prefixes (wcap/128 ints), then per
+// thread a staged a_ik (double) and four ints (cursor, end, flag, list), then
+// 64 ints of scratch.
 size_t heavy_win_smem_bytes(int threads, int vcap, int wcap_bits) {
-  return (size_t)vcap * 8 + (size_t)wcap_bits / 8 + (size_t)wcap_bits / 32 +
-         (size_t)threads * 20 + 64 * sizeof(int);
+  return (size_t)vcap * sizeof(double) + (size_t)wcap_bits / 32 * sizeof(uint32_t) +
+         (size_t)wcap_bits / 128 * sizeof(int) + (size_t)threads * sizeof(double) +
+         (size_t)threads * 4 * sizeof(int) + 64 * sizeof(int);
 }
 
 template <bool GRAM, int MAXT, int MINB>
