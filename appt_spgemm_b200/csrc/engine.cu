@@ -281,11 +281,12 @@ spg_config merged_config(const spg_config* user) {
   if (c.grid_sms < 0) c.grid_sms = 0;
   if (c.grid_sms > (1 << 16)) c.grid_sms = 1 << 16;
   if (c.small_max_nnz == 0) c.small_max_nnz = kSmallMaxNnzDefault;
-  if (c.dense_max_words == 0) c.dense_max_words = (int64_t)1 << kDenseMaxLog2W;
+  if (c.dense_max_words == 0) c.dense_max_words = -1;  // off unless asked for
   if (c.bin_streams <= 0) c.bin_streams = 4;
   if (c.bin_streams > spg_ctx::kMaxSides) c.bin_streams = spg_ctx::kMaxSides;
   if (c.dense_max_words > ((int64_t)1 << kDenseMaxLog2W))
     c.dense_max_words = (int64_t)1 << kDenseMaxLog2W;
+  if (c.heavy_vcap == 0) c.heavy_vcap = -1;  // in place in C unless asked for
   if (c.heavy_vcap > 0) {  // a power of two in [1024, 16384]
     int64_t v = 1024;
     while (v * 2 <= c.heavy_vcap && v < 16384) v *= 2;
@@ -995,8 +996,7 @@ spg_status execute_impl(spg_plan* p, spg_csr_out* C, cudaStream_t st) {
       // counts and cursors exist and the configuration allows it
       const bool shared_values = windows && ctx->cfg.heavy_vcap >= 0;
       const int win_threads = ctx->cfg.heavy_threads > 512 ? 1024 : 512;
-      h.vcap = ctx->cfg.heavy_vcap > 0 ? (int32_t)ctx->cfg.heavy_vcap
-                                       : (win_threads > 512 ? 16384 : 8192);
+      h.vcap = ctx->cfg.heavy_vcap > 0 ? (int32_t)ctx->cfg.heavy_vcap : 8192;
       h.wcap_bits = win_threads > 512 ? (1 << 18) : (1 << 17);
       cudaError_t e = cudaSuccess;
       if (windows) {

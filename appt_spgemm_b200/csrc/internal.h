@@ -38,6 +38,6 @@ constexpr int kDenseMinLog2W = 8;
 constexpr int kDenseMaxLog2W = 11;
 constexpr int kDenseBin0 = kHeavyBin + 1;     // 13
 constexpr int kNumBins = kDenseBin0 + kDenseMaxLog2W - kDenseMinLog2W + 1;  // 17
-constexpr int kDenseVals = 512;  // entries of a bitmap-path row (numeric)
+constexpr int kDenseVals = 256;  // entries of a bitmap-path row (numeric)
 
 }  // namespace spg

@@ -19,8 +19,10 @@
 //
 // Shared memory per warp: the bitmap (2^LOG2W words), a 16-bit prefix per word
 // and kDenseVals values (numeric).  Rows take this path when their span fits
-// 2^LOG2W words, the words are at most twice the products, and (numeric) the
-// row has at most kDenseVals entries (row_bin).
+// 2^LOG2W words, spans at most 8 columns per product, and (numeric) the row
+// has at most kDenseVals entries (row_bin).  Opt-in (spg_config.dense_max_words):
+// on the 27-point stencil, whose span is ~300 columns per output entry, the
+// bitmap's bookkeeping made it slower than the hash tables.
 #include <climits>
 
 #include "kernels.h"
@@ -76,7 +78,10 @@ __global__ void __launch_bounds__(256) k_dense_w32(RowArgs a) {
     __syncwarp();
     const int32_t ps = a.A.rowptr[row], pe = a.A.rowptr[row + 1];
 
-    // mark: segments in any order (an OR)
+    // mark: segments in any order (an OR); when every B row of a chunk fits
+    // one segment, the columns of kMarkAhead segments are loaded before any
+    // of them is marked (their loads overlap)
+    constexpr int kMarkAhead = 8;
     for (int32_t pb = ps; pb < pe; pb += 32) {
       const int cnt = min(32, pe - pb);
       int bs = 0, len = 0;
@@ -84,6 +89,20 @@ __global__ void __launch_bounds__(256) k_dense_w32(RowArgs a) {
         const int32_t k = a.A.col[pb + lane];
         bs = a.B.rowptr[k];
         len = a.B.rowptr[k + 1] - bs;
+      }
+      if (__all_sync(kFull, len <= 32)) {
+        for (int t0 = 0; t0 < cnt; t0 += kMarkAhead) {
+          int jr[kMarkAhead];
+#pragma unroll
+          for (int d = 0; d < kMarkAhead; ++d) {
+            const int t = t0 + d;
+            const int tb = __shfl_sync(kFull, bs, t & 31), tl = __shfl_sync(kFull, len, t & 31);
+            jr[d] = (t < cnt && lane < tl) ? a.B.col[tb + lane] : -1;
+          }
+#pragma unroll
+          for (int d = 0; d < kMarkAhead; ++d) mark_segment(bm, jr[d], lo);
+        }
+        continue;
       }
       for (int t = 0; t < cnt; ++t) {
         const int tb = __shfl_sync(kFull, bs, t), tl = __shfl_sync(kFull, len, t);

@@ -52,8 +52,8 @@ struct BinSource {
   int64_t short_split;
   int short_max_log2;
   int64_t short_min;
-  // rows whose output span fits 2^dense_max_log2w bitmap words, at most twice
-  // their products, with at least 64 products (and, numeric, at most
+  // rows whose output span fits 2^dense_max_log2w bitmap words and is at most
+  // 8 columns per product, with at least 64 products (and, numeric, at most
   // kDenseVals entries) take the bitmap bins; dense_max_log2w < kDenseMinLog2W:
   // never (the Gram path, or switched off)
   int dense_max_log2w;
@@ -89,7 +89,9 @@ __host__ __device__ __forceinline__ int row_bin(const BinSource& s, int i) {
     const int64_t f = s.f[i];
     // (symbolic: only rows the numeric binning can never send heavy, which
     // need the heavy symbolic kernel's block counts)
-    if (f >= 64 && words <= 2 * f && words <= ((int64_t)1 << s.dense_max_log2w) &&
+    // the bitmap's bookkeeping (clearing, counting, prefixes) grows with the
+    // span: worth it only where the span is at most 8 columns per product
+    if (f >= 64 && words * 4 <= f && words <= ((int64_t)1 << s.dense_max_log2w) &&
         (s.mode == 0 ? (s.short_split <= 0 || size < s.short_min) : size <= kDenseVals)) {
       int lw = ceil_log2_64(words);
       if (lw < kDenseMinLog2W) lw = kDenseMinLog2W;

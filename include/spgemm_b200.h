@@ -124,16 +124,20 @@ typedef struct spg_config {
                                  per phase); a row of more than 1536 products
                                  sends the plan to the regular path; 0 → 2^20,
                                  negative → never                               */
-  int64_t heavy_vcap;         /* heavy CTA rows: values held in shared memory per
-                                 column window (1024..16384, a power of two),
-                                 each window's values written to C once; 0 →
-                                 8192 (16384 with 1024-thread CTAs); negative →
-                                 accumulate in place in C (the dense-window
-                                 kernel, also taken without block counts)       */
-  int64_t dense_max_words;    /* rows whose output column span fits this many
-                                 32-bit bitmap words (256..2048) and is at most
-                                 twice their products take the bitmap kernels
-                                 (A·A, A·Aᵀ); 0 → 2048; negative → never        */
+  int64_t heavy_vcap;         /* heavy CTA rows: > 0 → values held in shared
+                                 memory per column window of at most this many
+                                 columns (1024..16384, a power of two), each
+                                 window's values written to C once; 0 or
+                                 negative → accumulated in place in C (the
+                                 dense-window kernel; the default: measured
+                                 faster on R-MAT, the windows multiply the
+                                 per-entry barriers)                            */
+  int64_t dense_max_words;    /* > 0 → rows whose output column span fits this
+                                 many 32-bit bitmap words (256..2048) and is at
+                                 most 8 columns per product take the bitmap
+                                 kernels (A·A, A·Aᵀ); 0 or negative → never (the
+                                 default: the hash tables measured faster on
+                                 the stencil)                                   */
   int32_t bin_streams;        /* the kernels of different row bins of one phase
                                  run concurrently on this many streams (forked
                                  from and joined back into the caller's

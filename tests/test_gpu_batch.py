@@ -150,7 +150,7 @@ def test_autotune_keeps_results_exact(eng):
                                    dict(num_load_pct=80, sym_load_pct=90, max_smem_slots=2048),
                                    dict(lanes_per_row=4, heavy_threads=256, window_bits=1 << 18),
                                    dict(grid_sms=1 << 16), dict(bin_streams=1),
-                                   dict(dense_max_words=-1, heavy_vcap=-1)])
+                                   dict(dense_max_words=2048, heavy_vcap=8192)])
 def test_tuning_knobs_preserve_results(knobs):
     from appt_spgemm_b200.engine import Engine
     with Engine("cuda:0", **knobs) as e:

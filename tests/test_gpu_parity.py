@@ -177,12 +177,23 @@ def test_one_readback_plan(eng):
         run_case(eng, B, task, "small/fallback")
 
 
-@pytest.mark.parametrize("words", [256, 512, 1024, -1])
+def strided(n, entries, step):
+    """Row i holds columns i + step·c, c = −entries..entries, inside [0, n):
+    C rows of 4·entries + 1 columns over a span of 4·entries·step."""
+    rows = [np.array([i + step * c for c in range(-entries, entries + 1)
+                      if 0 <= i + step * c < n], np.int32) for i in range(n)]
+    rp = np.concatenate([[0], np.cumsum([len(r) for r in rows])]).astype(np.int32)
+    val = np.random.default_rng(n + step).uniform(-1, 1, int(rp[-1]))
+    return csr.CsrHost(n, rp, np.concatenate(rows), val)
+
+
+@pytest.mark.parametrize("words", [256, 512, 1024, 2048, -1])
 def test_dense_bitmap_rows(words):
-    """Rows over a bitmap of their output span (bitmap bins of up to 256, 512
-    and 1024 words, or switched off): stencils, banded matrices and a random
-    graph (whose spans are too wide, so it stays on the hash tables), all
-    tasks (the Gram path never takes the bitmap bins)."""
+    """Rows over a bitmap of their output span (bitmap bins of up to 256, 512,
+    1024 and 2048 words, or switched off): stencils, banded matrices, rows of
+    far-apart columns (spans of 375 and 563 words) and a random graph (whose
+    spans are too wide, so it stays on the hash tables), all tasks (the Gram
+    path never takes the bitmap bins)."""
     from appt_spgemm_b200.engine import Engine
     cases = [(csr.stencil27(12, 5), "st12"), (csr.stencil27(30, 6), "st30"),
              (csr.banded(3000, 30, 0.3, 7), "band30"), (csr.banded(20000, 64, 0.3, 8), "band64"),
@@ -191,9 +202,10 @@ def test_dense_bitmap_rows(words):
         for A, lab in cases:
             for task in TASKS:
                 run_case(e, A, task, f"dense{words}/{lab}")
-        # spans of 458 and 521 words: the 512- and 1024-word bins
-        for A, lab in ((csr.stencil27(60, 11), "st60"), (csr.stencil27(64, 12), "st64")):
-            run_case(e, A, "AA", f"dense{words}/{lab}")
+        # 61 entries 100 or 150 columns apart: the 512- and 1024-word bins
+        for A, lab in ((strided(30000, 30, 100), "far100"), (strided(30000, 30, 150), "far150")):
+            for task in ("AA", "AAt"):
+                run_case(e, A, task, f"dense{words}/{lab}")
         e.check_device_status()
 
 
