@@ -282,8 +282,8 @@ spg_config merged_config(const spg_config* user) {
   if (c.grid_sms > (1 << 16)) c.grid_sms = 1 << 16;
   if (c.small_max_nnz == 0) c.small_max_nnz = kSmallMaxNnzDefault;
   if (c.dense_max_words == 0) c.dense_max_words = -1;  // off unless asked for
-  if (c.bin_streams <= 0) c.bin_streams = 4;
-  if (c.bin_streams > spg_ctx::kMaxSides) c.bin_streams = spg_ctx::kMaxSides;
+  if (c.bin_streams <= 0) c.bin_streams = 1;  // one stream unless asked for
+  if (c.bin_streams > 4) c.bin_streams = 4;
   if (c.dense_max_words > ((int64_t)1 << kDenseMaxLog2W))
     c.dense_max_words = (int64_t)1 << kDenseMaxLog2W;
   if (c.heavy_vcap == 0) c.heavy_vcap = -1;  // in place in C unless asked for
@@ -1103,8 +1103,8 @@ spg_status spg_create(spg_ctx** out, const spg_config* cfg) {
       st = cuda_status(e, "event");
       break;
     }
-    for (int i = 0; i < spg_ctx::kMaxSides && i < ctx->cfg.bin_streams && ctx->cfg.bin_streams > 1;
-         ++i) {
+    // side streams for concurrent bins (bin_streams > 1 at creation or later)
+    for (int i = 0; i < 4; ++i) {
       if ((e = cudaStreamCreateWithFlags(&ctx->side[i], cudaStreamNonBlocking)) != cudaSuccess ||
           (e = cudaEventCreateWithFlags(&ctx->side_done[i], cudaEventDisableTiming)) != cudaSuccess) {
         st = cuda_status(e, "side stream");

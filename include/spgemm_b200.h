@@ -138,10 +138,13 @@ typedef struct spg_config {
                                  kernels (A·A, A·Aᵀ); 0 or negative → never (the
                                  default: the hash tables measured faster on
                                  the stencil)                                   */
-  int32_t bin_streams;        /* the kernels of different row bins of one phase
-                                 run concurrently on this many streams (forked
-                                 from and joined back into the caller's
-                                 stream); 0 → 4; 1 → all on the caller's stream */
+  int32_t bin_streams;        /* > 1 → the kernels of different row bins of one
+                                 phase run concurrently on up to this many
+                                 streams (at most 4, forked from and joined back
+                                 into the caller's stream); 0 or 1 → all on the
+                                 caller's stream (the default: running the bins
+                                 at once measured slower, their persistent
+                                 grids contend for the SMs)                     */
   int32_t pad0;
 } spg_config;
 

@@ -149,7 +149,7 @@ def test_autotune_keeps_results_exact(eng):
 @pytest.mark.parametrize("knobs", [dict(num_load_pct=40, sym_load_pct=50),
                                    dict(num_load_pct=80, sym_load_pct=90, max_smem_slots=2048),
                                    dict(lanes_per_row=4, heavy_threads=256, window_bits=1 << 18),
-                                   dict(grid_sms=1 << 16), dict(bin_streams=1),
+                                   dict(grid_sms=1 << 16), dict(bin_streams=4),
                                    dict(dense_max_words=2048, heavy_vcap=8192)])
 def test_tuning_knobs_preserve_results(knobs):
     from appt_spgemm_b200.engine import Engine
