@@ -5,9 +5,10 @@
 // The reference's run_ours (src/spgemm_engine.cuh:132-210) allocates and frees
 // every buffer per call, issues at least two blocking 8-byte device→host copies
 // per phase and hands C to nobody.  Here workspace comes from a per-context
-// stream-ordered memory pool, the plan makes three host synchronisations
-// (input validation, bin sizes, nnz(C)), and execute is fully asynchronous and
-// writes C into caller-visible CSR arrays.
+// stream-ordered memory pool, the plan makes two host synchronisations (the
+// validation verdict with the bin sizes, then nnz(C); one for small matrices),
+// and execute is fully asynchronous and writes C into caller-visible CSR
+// arrays.
 #include <cuda_runtime.h>
 
 #include <chrono>
@@ -370,7 +371,7 @@ spg_status check_matrix(const spg_csr_dev* A) {
   return SPG_OK;
 }
 
-// Validate A on the device and wait for the verdict (host sync #1).
+// Validate A on the device and wait for the verdict (spg_describe).
 // When sym_tval is given, the values of Aᵀ for a structurally symmetric A are
 // gathered in the same round trip and *symmetric tells whether that held.
 spg_status validate_device(spg_ctx* ctx, const MatView& A, cudaStream_t st,
@@ -604,20 +605,28 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
   p->info.n = n;
   p->info.task = p->task;
   p->info.nnz_a = Ad->nnz;
-  // B = A; or Aᵀ: for a structurally symmetric A only its values move (gathered
-  // during validation), otherwise the counting-sort transpose builds it
+  // B = A; or Aᵀ: for a structurally symmetric A only its values move, gathered
+  // here; otherwise the counting-sort transpose builds it.  Nothing waits for
+  // the validation verdict or the symmetry check: the pre-pass and the binning
+  // check every index they use, and the verdict and the check come back with
+  // the bin sizes (sync #1 of the plan); an A·Aᵀ whose pattern turns out not
+  // to be symmetric is then transposed and binned again (one more sync).
   double* bx = nullptr;
-  bool symmetric = false;
   if (p->task != SPG_TASK_AA) TRY(palloc(p, &bx, Ad->nnz));
-  TRY(validate_device(ctx, p->A, st, bx, bx ? &symmetric : nullptr));
-  p->info.symmetric_pattern = symmetric ? 1 : 0;
-  p->symmetric = symmetric;
+  TRY_CUDA(cudaMemsetAsync(ctx->d_status, 0, 2 * sizeof(uint32_t), st), "status reset");
+  {
+    ProfScope ps(ctx, "plan/validate", st);
+    TRY_CUDA(launch_validate(p->A, ctx->d_status, st), "validate");
+  }
+  if (bx) {
+    ProfScope ps(ctx, "plan/transpose_sym", st);
+    TRY_CUDA(launch_sym_transpose_vals(p->A, bx, (int*)(ctx->d_status + 1), st),
+             "symmetric transpose");
+  }
   p->bt_val = bx;
-  if (p->task == SPG_TASK_AA) {
-    p->B = p->A;
-  } else if (symmetric) {
-    p->B = MatView{n, Ad->nnz, Ad->rowptr, Ad->col, bx};
-  } else {
+  p->symmetric = p->task != SPG_TASK_AA;  // until the check says otherwise
+  p->B = p->task == SPG_TASK_AA ? p->A : MatView{n, Ad->nnz, Ad->rowptr, Ad->col, bx};
+  auto build_transpose = [&]() -> spg_status {
     int32_t *bp, *bi;
     TRY(palloc(p, &bp, (int64_t)n + 1));
     TRY(palloc(p, &bi, Ad->nnz));
@@ -638,7 +647,9 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
     p->tw = w;
     p->bt_rowptr = bp;
     p->bt_col = bi;
-  }
+    p->symmetric = false;
+    return SPG_OK;
+  };
 
   // lanes per row in the sub-warp bins: next power of two of B's mean row length
   if (ctx->cfg.lanes_per_row > 0) {
@@ -650,15 +661,11 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
     p->G = g;
   }
 
-  // pre-pass and symbolic binning (host sync #2: bin sizes)
+  // pre-pass and symbolic binning (host sync #1: verdict, symmetry, bin sizes)
   TRY(palloc(p, &p->f, n));
   TRY(palloc(p, &p->lo, n));
   TRY(palloc(p, &p->hi, n));
   TRY(palloc(p, &p->hqueue, kNumBins));
-  {
-    ProfScope ps(ctx, "plan/prepass", st);
-    TRY_CUDA(launch_prepass(p->A, p->B, p->f, p->lo, p->hi, st), "prepass");
-  }
   const int nblocks = (n + kBinRowsPerBlock - 1) / kBinRowsPerBlock;
   int32_t* hist;
   int64_t* counts;
@@ -685,10 +692,6 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
                  numeric_heavy_min(num_lg, ctx->cfg.num_load_pct),
                  p->A.rowptr, split, short_lg,
                  numeric_heavy_min(short_lg, ctx->cfg.num_load_pct), dense_lw};
-  {
-    ProfScope ps(ctx, "plan/bin_sym", st);
-    TRY_CUDA(launch_bin_rows(bsym, hist, counts, rows_sym, st), "symbolic binning");
-  }
   // column blocks of the heavy rows: 1024 columns (windows are packed from
   // the counts; a block above the window cap, 675 columns at the default
   // load, is cut into fixed 512-column windows); wider when that many counts
@@ -700,16 +703,41 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
   TRY(palloc(p, &nblk, n));
   TRY(palloc(p, &p->blk_off, (int64_t)n + 1));
   TRY(palloc(p, (char**)&btmp, (int64_t)scan_tmp_bytes(n)));
-  {
-    ProfScope ps(ctx, "plan/heavy_blocks", st);
-    TRY_CUDA(launch_heavy_blocks(bsym, p->blk_log2, nblk, p->blk_off, btmp, st), "heavy blocks");
-  }
   int64_t* hp = p->ctx->h_pin;
-  TRY_CUDA(cudaMemcpyAsync(hp, counts, sizeof(int64_t) * 2 * kNumBins, cudaMemcpyDeviceToHost, st),
-           "bin readback");
-  TRY_CUDA(cudaMemcpyAsync(hp + 2 * kNumBins, p->blk_off + n, sizeof(int64_t),
-                           cudaMemcpyDeviceToHost, st), "bin readback");
-  TRY_CUDA(cudaStreamSynchronize(st), "bin sync");
+  // pre-pass, binning and block offsets over the current B, then one readback
+  // of the bin sizes, the heavy blocks' total and the two status words
+  auto bin_pass = [&]() -> spg_status {
+    {
+      ProfScope ps(ctx, "plan/prepass", st);
+      TRY_CUDA(launch_prepass(p->A, p->B, p->f, p->lo, p->hi, st), "prepass");
+    }
+    {
+      ProfScope ps(ctx, "plan/bin_sym", st);
+      TRY_CUDA(launch_bin_rows(bsym, hist, counts, rows_sym, st), "symbolic binning");
+    }
+    {
+      ProfScope ps(ctx, "plan/heavy_blocks", st);
+      TRY_CUDA(launch_heavy_blocks(bsym, p->blk_log2, nblk, p->blk_off, btmp, st),
+               "heavy blocks");
+    }
+    TRY_CUDA(cudaMemcpyAsync(hp, counts, sizeof(int64_t) * 2 * kNumBins, cudaMemcpyDeviceToHost,
+                             st), "bin readback");
+    TRY_CUDA(cudaMemcpyAsync(hp + 2 * kNumBins, p->blk_off + n, sizeof(int64_t),
+                             cudaMemcpyDeviceToHost, st), "bin readback");
+    TRY_CUDA(cudaMemcpyAsync(hp + 2 * kNumBins + 1, ctx->d_status, 2 * sizeof(uint32_t),
+                             cudaMemcpyDeviceToHost, st), "status readback");
+    TRY_CUDA(cudaStreamSynchronize(st), "bin sync");
+    const uint32_t* words = (const uint32_t*)(hp + 2 * kNumBins + 1);
+    if (words[0] & DEV_ERR_INVALID_CSR) return status_from_bits(DEV_ERR_INVALID_CSR);
+    return SPG_OK;
+  };
+  TRY(bin_pass());
+  if (p->symmetric && ((const uint32_t*)(hp + 2 * kNumBins + 1))[1] != 0) {
+    // A·Aᵀ of a pattern that is not symmetric: transpose and bin again
+    TRY(build_transpose());
+    TRY(bin_pass());
+  }
+  p->info.symmetric_pattern = p->symmetric ? 1 : 0;
   int64_t sym_count[kNumBins], sym_start[kNumBins];
   for (int b = 0; b < kNumBins; ++b) {
     sym_count[b] = hp[b];
@@ -806,7 +834,7 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
     TRY_CUDA(launch_scan_i32_i64(p->rowlow, p->lowptr, n, scan_tmp2, st), "lower scan");
   }
 
-  // numeric binning by exact counts, stats; host sync #3 (nnz(C))
+  // numeric binning by exact counts, stats; host sync #2 (nnz(C))
   TRY(palloc(p, &p->rows_num, n));
   BinSource bnum{1, n, p->f, p->lo, p->hi, p->rownnz, gram ? p->rowlow : nullptr, num_lg, force,
                  ctx->cfg.num_load_pct, 0, p->A.rowptr, split, short_lg, 0, dense_lw};

@@ -209,10 +209,12 @@ spg_status spg_destroy(spg_ctx* ctx);
 spg_status spg_check_device_status(spg_ctx* ctx, void* stream);
 
 /* ---- plan / execute (replaces the sizing half of run_ours) ---------------- */
-/* Pre-pass + binning + symbolic phase.  Three host synchronisations, each a
- * small pinned readback: the validity verdict on A, the bin sizes, nnz(C);
- * one (verdict, nnz(C) and row statistics together) for the small matrices
- * of spg_config.small_max_nnz.
+/* Pre-pass + binning + symbolic phase.  Two host synchronisations, each a
+ * small pinned readback: the validity verdict on A with the bin sizes (and,
+ * for A·Aᵀ, whether A's pattern is symmetric), then nnz(C); a third when an
+ * A·Aᵀ pattern turns out not to be symmetric (it is transposed and binned
+ * again); one (verdict, nnz(C) and row statistics together) for the small
+ * matrices of spg_config.small_max_nnz.
  * When it returns, no kernel of the plan's symbolic phase is still running.
  * A must stay valid until the plan is destroyed. */
 spg_status spg_plan_create(spg_ctx* ctx, spg_task task, const spg_csr_dev* A,
