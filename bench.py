@@ -80,6 +80,8 @@ def parse_args():
                     help="requests per arrival rate in --mode serve")
     ap.add_argument("--serve-rates", default="50,500,5000")
     ap.add_argument("--serve-pool", type=int, default=40, help="distinct matrices in the pool")
+    ap.add_argument("--serve-workers", type=int, default=0,
+                    help="workers of the continuous-batching server (0: its default)")
     ap.add_argument("--serve-seeds", type=int, default=1,
                     help="arrival streams per rate in --mode serve (each run through both "
                          "servers); figures are medians over the streams")
@@ -684,6 +686,8 @@ def run_serve(args):
             tasks = np.where(rng.random(nreq) < 0.5, "AA", "AAt")
             gaps = rng.exponential(1.0 / rate, nreq)
             for label, kw in SERVERS:
+                if label == "continuous_batching" and args.serve_workers > 0:
+                    kw = dict(kw, workers=args.serve_workers)
                 r = serve_once(pool, ds, prods, rate, label, kw, picks, tasks, gaps)
                 runs.setdefault((rate, label), []).append(r)
                 print(json.dumps(dict(r, stream=stream)), file=sys.stderr, flush=True)
