@@ -502,10 +502,6 @@ spg_status plan_build_small(spg_plan* p, const spg_csr_dev* Ad, bool* fallback) 
   p->hqueue = (int32_t*)(w + o_q);
   unsigned long long* stats = (unsigned long long*)(w + o_stats);
   TRY_CUDA(cudaMemsetAsync(ctx->d_status, 0, 2 * sizeof(uint32_t), st), "status reset");
-  {
-    ProfScope ps(ctx, "plan/validate", st);
-    TRY_CUDA(launch_validate(p->A, ctx->d_status, st), "validate");
-  }
   if (aat) {
     TransposeWork tw{};
     tw.cnt = (int32_t*)(w + o_tc);
@@ -530,9 +526,9 @@ spg_status plan_build_small(spg_plan* p, const spg_csr_dev* Ad, bool* fallback) 
   } else {
     p->B = p->A;
   }
-  {
+  {  // the pre-pass also validates A
     ProfScope ps(ctx, "plan/prepass", st);
-    TRY_CUDA(launch_prepass(p->A, p->B, p->f, p->lo, p->hi, st), "prepass");
+    TRY_CUDA(launch_prepass(p->A, p->B, p->f, p->lo, p->hi, st, ctx->d_status), "prepass");
   }
   RowArgs ra{};
   ra.A = p->A;
@@ -614,10 +610,6 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
   double* bx = nullptr;
   if (p->task != SPG_TASK_AA) TRY(palloc(p, &bx, Ad->nnz));
   TRY_CUDA(cudaMemsetAsync(ctx->d_status, 0, 2 * sizeof(uint32_t), st), "status reset");
-  {
-    ProfScope ps(ctx, "plan/validate", st);
-    TRY_CUDA(launch_validate(p->A, ctx->d_status, st), "validate");
-  }
   if (bx) {
     ProfScope ps(ctx, "plan/transpose_sym", st);
     TRY_CUDA(launch_sym_transpose_vals(p->A, bx, (int*)(ctx->d_status + 1), st),
@@ -707,9 +699,9 @@ spg_status plan_build(spg_plan* p, const spg_csr_dev* Ad) {
   // pre-pass, binning and block offsets over the current B, then one readback
   // of the bin sizes, the heavy blocks' total and the two status words
   auto bin_pass = [&]() -> spg_status {
-    {
+    {  // the pre-pass also validates A (the verdict comes back below)
       ProfScope ps(ctx, "plan/prepass", st);
-      TRY_CUDA(launch_prepass(p->A, p->B, p->f, p->lo, p->hi, st), "prepass");
+      TRY_CUDA(launch_prepass(p->A, p->B, p->f, p->lo, p->hi, st, ctx->d_status), "prepass");
     }
     {
       ProfScope ps(ctx, "plan/bin_sym", st);

@@ -52,22 +52,29 @@ cudaError_t launch_validate(const MatView& A, uint32_t* status, cudaStream_t s) 
 // pre-pass: products and output column span per row (one warp per row)
 // ---------------------------------------------------------------------------
 // Every index is checked before it is used, so the kernel may run before the
-// host has seen the validation verdict (the one-readback plan): a row that
-// meets a row pointer or column outside its range gets f = −1, and the later
-// kernels of that plan skip it.
+// host has seen the validation verdict: a row that meets a row pointer or
+// column outside its range gets f = −1, and the later kernels of the
+// one-readback plan skip it.  With `status` set it is also the validation of
+// A (k_validate's checks, in the same read of A's rows): a violation sets
+// DEV_ERR_INVALID_CSR there.
 __global__ void k_prepass(MatView A, MatView B, int64_t* __restrict__ f, int32_t* __restrict__ lo,
-                          int32_t* __restrict__ hi) {
+                          int32_t* __restrict__ hi, uint32_t* status) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  if (status && warp == 0 && lane == 0 &&
+      (A.rowptr[0] != 0 || (int64_t)A.rowptr[A.n] != A.nnz))
+    report(status, DEV_ERR_INVALID_CSR);
   for (int64_t i = warp; i < A.n; i += nwarps) {
     int32_t s = A.rowptr[i], e = A.rowptr[i + 1];
     bool bad = s < 0 || e < s || (int64_t)e > A.nnz;
     if (bad) s = e = 0;
     long long prod = 0;
     int mn = INT_MAX, mx = -1;
+    bool unsorted = false;
     for (int32_t p = s + lane; p < e; p += 32) {
       const int32_t k = A.col[p];
+      if (status && p > s && A.col[p - 1] >= k) unsorted = true;
       if (k < 0 || k >= B.n) {
         bad = true;
         continue;
@@ -89,6 +96,8 @@ __global__ void k_prepass(MatView A, MatView B, int64_t* __restrict__ f, int32_t
       mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     }
     bad = __any_sync(0xffffffffu, bad);
+    unsorted = __any_sync(0xffffffffu, unsorted);
+    if (status && lane == 0 && (bad || unsorted)) report(status, DEV_ERR_INVALID_CSR);
     if (lane == 0) {
       f[i] = bad ? -1 : prod;
       lo[i] = bad ? INT_MAX : mn;
@@ -98,12 +107,16 @@ __global__ void k_prepass(MatView A, MatView B, int64_t* __restrict__ f, int32_t
 }
 
 cudaError_t launch_prepass(const MatView& A, const MatView& B, int64_t* f, int32_t* lo,
-                           int32_t* hi, cudaStream_t s) {
-  if (A.n == 0) return cudaSuccess;
+                           int32_t* hi, cudaStream_t s, uint32_t* status) {
+  if (A.n == 0) {
+    if (!status) return cudaSuccess;
+    // no rows: the validation is rowptr[0] == 0 and nnz == 0 alone
+    return launch_validate(A, status, s);
+  }
   const int threads = 256;
   int64_t blocks = ((int64_t)A.n * 32 + threads - 1) / threads;
   if (blocks > 148 * 64) blocks = 148 * 64;
-  k_prepass<<<(unsigned)blocks, threads, 0, s>>>(A, B, f, lo, hi);
+  k_prepass<<<(unsigned)blocks, threads, 0, s>>>(A, B, f, lo, hi, status);
   SPG_COUNT_LAUNCH();
   return cudaGetLastError();
 }

@@ -23,9 +23,10 @@ cudaError_t launch_validate(const MatView& A, uint32_t* status, cudaStream_t s);
 
 // Per row i of C = A·B: products f_i = Σ_{k∈A_i} nnz(B_k) and the column span
 // [lo_i, hi_i] of the output row (B rows sorted).  Rows with f_i = 0 get
-// lo = INT_MAX, hi = -1.
+// lo = INT_MAX, hi = -1; rows that meet an index out of range f_i = −1.  With
+// `status`, A is validated in the same pass (launch_validate's checks).
 cudaError_t launch_prepass(const MatView& A, const MatView& B, int64_t* f, int32_t* lo,
-                           int32_t* hi, cudaStream_t s);
+                           int32_t* hi, cudaStream_t s, uint32_t* status = nullptr);
 
 // What a row's bin is computed from.
 struct BinSource {
