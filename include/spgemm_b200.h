@@ -354,7 +354,8 @@ spg_status spg_free(spg_ctx* ctx, void* dev_ptr, void* stream);
 /* ---- profiling ------------------------------------------------------------ */
 /* Per-kernel CUDA events recorded on the launching stream (off by default) and
  * a count of the engine's kernel launches on the calling thread.
- * spg_profile_read synchronises the device and writes JSON text
+ * spg_profile_read waits for the recorded kernels (their end events, not the
+ * whole device) and writes JSON text
  *   {"launches": L, "kernels": {"<phase>/<kernel>": {"count": c, "ms": t}, ...}}
  * covering the calls since the last spg_profile_reset. */
 spg_status spg_profile_enable(spg_ctx* ctx, int32_t enable);
