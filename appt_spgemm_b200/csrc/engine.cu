@@ -548,9 +548,9 @@ spg_status plan_build_small(spg_plan* p, const spg_csr_dev* Ad, bool* fallback) 
   }
   {
     ProfScope ps(ctx, "plan/scan", st);
-    TRY_CUDA(launch_scan_i32_i64(p->rownnz, p->rowptr, n, w + o_scan, st), "row pointer scan");
+    TRY_CUDA(launch_scan_stats_small(p->rownnz, p->f, n, p->rowptr, stats, w + o_scan, st),
+             "row pointer scan");
   }
-  TRY_CUDA(launch_row_stats(p->f, p->rownnz, n, stats, st), "row stats");
   int64_t* hp = ctx->h_pin;
   TRY_CUDA(cudaMemcpyAsync(hp, ctx->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, st),
            "readback");

@@ -320,6 +320,78 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_single(const int32_t* __r
   if (threadIdx.x == 0) out[n] = (OutT)tot;
 }
 
+// One tile: the row-pointer scan and the row statistics (Σ products, max
+// products, max row count) of a small plan in a single launch.
+__global__ void __launch_bounds__(kScanThreads) k_scan_stats_single(
+    const int32_t* __restrict__ cnt, const int64_t* __restrict__ f, int64_t n,
+    int64_t* __restrict__ rowptr, unsigned long long* __restrict__ stats) {
+  __shared__ long long scratch[32];
+  __shared__ unsigned long long red[3][32];
+  const int64_t base = (int64_t)threadIdx.x * kScanItems;
+  int32_t v[kScanItems];
+  long long s = 0;
+  unsigned long long sf = 0, mf = 0, mc = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    const bool in = base + k < n;
+    v[k] = in ? cnt[base + k] : 0;
+    s += v[k];
+    if (in) {
+      const unsigned long long fk = (unsigned long long)f[base + k];
+      sf += fk;
+      mf = fk > mf ? fk : mf;
+      const unsigned long long ck = (unsigned long long)v[k];
+      mc = ck > mc ? ck : mc;
+    }
+  }
+  long long tot;
+  long long run = block_exclusive_scan64(s, scratch, &tot);
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    if (base + k < n) rowptr[base + k] = run;
+    run += v[k];
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    sf += __shfl_xor_sync(0xffffffffu, sf, o);
+    const unsigned long long a = __shfl_xor_sync(0xffffffffu, mf, o);
+    const unsigned long long b = __shfl_xor_sync(0xffffffffu, mc, o);
+    mf = a > mf ? a : mf;
+    mc = b > mc ? b : mc;
+  }
+  const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    red[0][w] = sf;
+    red[1][w] = mf;
+    red[2][w] = mc;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long a = 0, b = 0, c = 0;
+    for (int i = 0; i < nw; ++i) {
+      a += red[0][i];
+      b = red[1][i] > b ? red[1][i] : b;
+      c = red[2][i] > c ? red[2][i] : c;
+    }
+    stats[0] = a;
+    stats[1] = b;
+    stats[2] = c;
+    rowptr[n] = tot;
+  }
+}
+
+cudaError_t launch_scan_stats_small(const int32_t* cnt, const int64_t* f, int64_t n,
+                                    int64_t* rowptr, unsigned long long* stats, void* tmp,
+                                    cudaStream_t s) {
+  if (n <= 0 || n > kScanTile) {
+    cudaError_t e = launch_scan_i32_i64(cnt, rowptr, n, tmp, s);
+    if (e != cudaSuccess) return e;
+    return launch_row_stats(f, cnt, (int32_t)n, stats, s);
+  }
+  k_scan_stats_single<<<1, kScanThreads, 0, s>>>(cnt, f, n, rowptr, stats);
+  SPG_COUNT_LAUNCH();
+  return cudaGetLastError();
+}
+
 size_t scan_tmp_bytes(int64_t n) {
   int64_t ntiles = (n + kScanTile - 1) / kScanTile;
   return sizeof(long long) * (size_t)(ntiles + 1);

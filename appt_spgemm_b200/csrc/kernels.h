@@ -366,6 +366,11 @@ cudaError_t launch_describe(const MatView& A, const int32_t* colcount, DescAccum
 // out[0] = Σ f, out[1] = max f, out[2] = max rownnz (out zeroed by the launcher).
 cudaError_t launch_row_stats(const int64_t* f, const int32_t* rownnz, int32_t n,
                              unsigned long long* out, cudaStream_t s);
+// Row pointers of a small plan and its row statistics: one launch when n fits
+// one scan tile, else the scan and launch_row_stats.
+cudaError_t launch_scan_stats_small(const int32_t* cnt, const int64_t* f, int64_t n,
+                                    int64_t* rowptr, unsigned long long* stats, void* tmp,
+                                    cudaStream_t s);
 cudaError_t launch_col_count(const MatView& A, int32_t* cnt, cudaStream_t s);
 
 }  // namespace spg

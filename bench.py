@@ -752,6 +752,15 @@ def laplace_subresult(eng, reps=50):
         m["nnz_c"] = pl.nnz_c
         pl.close()
         out["ours"][task] = m
+    # the same calls through the reference-compatible C entry point: spg_run_ours
+    # times `reps` full calls with CUDA events in C++, as the reference's
+    # run_ours does (src/spgemm_engine.cuh:199-202), with no Python in the loop
+    from appt_spgemm_b200.engine import run_ours
+    out["ours_run_ours"] = {}
+    for task in ("AA", "AAt"):
+        r = run_ours(task, dA.rowptr, dA.col, dA.val, A.n, A.nnz, reps)
+        out["ours_run_ours"][task] = {"ms_mean": round(r.ms, 4),
+                                      "us_per_call": round(1e3 * r.ms, 1), "nnz_c": r.nnz}
     out["cusparse"] = cusparse_baseline(dA, A, prods["AA"], prods["AAt"], reps=20)
     out["reference_gpu_engine"] = reference_gpu_baseline(A, prods["AA"], prods["AAt"], reps=20)
     for k in ("cusparse", "reference_gpu_engine"):
