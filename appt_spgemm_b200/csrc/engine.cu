@@ -576,9 +576,19 @@ spg_status plan_build_small(spg_plan* p, const spg_csr_dev* Ad, bool* fallback) 
   p->info.heavy_rows = 0;
   p->info.bins_used = 1;
   p->info.symmetric_pattern = 0;
-  // numeric table: the exact largest row at the numeric load, 64 to 2048 slots
+  // numeric table: the exact largest row at the numeric load, 16 to 2048
+  // slots; tables below 2048 slots run rows on lane groups sized to B's mean
+  // row length (several rows per warp), 2048 a warp per row
   int lg = ceil_log2_64((int64_t)sv[2] * 100 / ctx->cfg.num_load_pct + 1);
-  p->small_log2 = lg < 6 ? 6 : (lg > 11 ? 11 : lg);
+  p->small_log2 = lg < kMinTableLog2 ? kMinTableLog2 : (lg > 11 ? 11 : lg);
+  if (ctx->cfg.lanes_per_row > 0) {
+    p->G = ctx->cfg.lanes_per_row;
+  } else {
+    const double mean = n > 0 ? (double)nnz / n : 1.0;
+    int g = 4;
+    while (g < 32 && g < mean) g <<= 1;
+    p->G = g;
+  }
   p->info.output_bytes = 8 * ((int64_t)n + 1) + 12 * p->nnz_c;
   p->info.workspace_bytes = p->ws_bytes;
   p->info.exec_workspace_bytes = 0;
@@ -960,9 +970,10 @@ spg_status execute_impl(spg_plan* p, spg_csr_out* C, cudaStream_t st) {
       RowArgs r = ra;
       r.rows = nullptr;
       r.nrows = n;
-      r.G = 32;
+      const int bin = p->small_log2 - kMinTableLog2 + 1;
+      r.G = hash_bin_lanes(bin, p->G);
       ProfScope ps(ctx, "num/small", st);
-      cudaError_t e = launch_hash_w32(p->small_log2, true, false, r, ctx->num_sms, st);
+      cudaError_t e = launch_hash_bin(bin, true, false, r, ctx->num_sms, st);
       if (e != cudaSuccess) result = cuda_status(e, "numeric");
     }
     for (int b = 1; b <= kNumTableBins && result == SPG_OK; ++b) {

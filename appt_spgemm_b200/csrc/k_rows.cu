@@ -241,8 +241,8 @@ __global__ void __launch_bounds__(256) k_hash_warp(RowArgs a) {
   }
   st_len = st_bs + a.G;
   for (int r = blockIdx.x * rows_per_cta + gi; r < a.nrows; r += gridDim.x * rows_per_cta)
-    hash_row<LOG2T, NUMERIC, GRAM>(g, a, a.rows[r], keys, vals, st_bs, st_len, st_a, nullptr,
-                                   nullptr, nullptr);
+    hash_row<LOG2T, NUMERIC, GRAM>(g, a, a.rows ? a.rows[r] : r, keys, vals, st_bs, st_len,
+                                   st_a, nullptr, nullptr, nullptr);
 }
 
 template <int LOG2T, bool NUMERIC, bool GRAM>
