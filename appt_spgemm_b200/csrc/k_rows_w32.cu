@@ -129,24 +129,6 @@ __device__ __noinline__ void pair_sort_write(const RowArgs& a, int row, int* key
   }
 }
 
-// Symbolic insert into a table of 2^lg slots chosen per row (lg <= the
-// kernel's LOG2T): the one-readback plan runs every row through one launch
-// with the largest table, and sizes each row's share to its products.
-__device__ __forceinline__ void insert_key_rt(int* keys, int j, int lg, uint32_t* status) {
-  const unsigned T = 1u << lg;
-  unsigned h = ((unsigned)j * 0x9E3779B1u) >> (32 - lg);
-  int old = atomicCAS(keys + h, kEmptyKey, j);
-  unsigned probe = 1;
-  while (old != kEmptyKey && old != j) {
-    if (probe++ == T) {
-      report(status, DEV_ERR_HASH_FULL);
-      return;
-    }
-    h = (h + 1) & (T - 1);
-    old = atomicCAS(keys + h, kEmptyKey, j);
-  }
-}
-
 }  // namespace
 
 // Five CTAs of 256 threads per SM (48 registers, no spills).  Measured on the
@@ -169,10 +151,6 @@ __global__ void __launch_bounds__(256, 5) k_hash_w32(RowArgs a) {
 
   for (int r = blockIdx.x * nw + w; r < a.nrows; r += gridDim.x * nw) {
     const int row = a.rows ? a.rows[r] : r;
-    // table slots this row uses: all of them, except in the one-readback
-    // plan's symbolic launch, where a row takes 2^lg slots for its products
-    // (min(products, span) at 75% load, at least 64)
-    int lg = LOG2T;
     if (!NUMERIC && a.fsmall) {
       const int64_t fr = a.fsmall[row];
       if (fr < 0 || fr > a.fcap) {
@@ -183,13 +161,11 @@ __global__ void __launch_bounds__(256, 5) k_hash_w32(RowArgs a) {
         }
         continue;
       }
-      const int64_t span = (int64_t)a.hi[row] - a.lo[row] + 1;
-      const int64_t need = (fr < span ? fr : span) * 4 / 3 + 1;
-      lg = 6;
-      while (lg < LOG2T && ((int64_t)1 << lg) < need) ++lg;
     }
-    const bool rt = !NUMERIC && lg < LOG2T;  // warp-uniform
-    for (int s = lane * 4; s < (1 << lg); s += 128) *(int4*)(keys + s) = make_int4(-1, -1, -1, -1);
+    // (a table sized per row to its products here, at 75% or 50% load, measured
+    // slower on random-graph rows, whose products are nearly all distinct: 512
+    // plain calls of the batch mix 224 / 204 ms against 191 ms)
+    for (int s = lane * 4; s < T; s += 128) *(int4*)(keys + s) = make_int4(-1, -1, -1, -1);
     __syncwarp();
     const int32_t ps = a.A.rowptr[row], pe = a.A.rowptr[row + 1];
     for (int32_t pb = ps; pb < pe; pb += 32) {
@@ -223,9 +199,8 @@ __global__ void __launch_bounds__(256, 5) k_hash_w32(RowArgs a) {
           for (int d = 0; d < D; ++d) {
             const int j = jr[d];
             if (j >= 0 && !(NUMERIC && GRAM && j < row)) {
-              if (rt) insert_key_rt(keys, j, lg, a.status);
-              else insert_acc<LOG2T, NUMERIC>(keys, vals, j, NUMERIC ? __dmul_rn(ar[d], br[d]) : 0.0,
-                                              a.status);
+              insert_acc<LOG2T, NUMERIC>(keys, vals, j, NUMERIC ? __dmul_rn(ar[d], br[d]) : 0.0,
+                                         a.status);
             }
             if (NUMERIC) __syncwarp();  // k-order of the accumulation
           }
@@ -274,9 +249,8 @@ __global__ void __launch_bounds__(256, 5) k_hash_w32(RowArgs a) {
         for (int d = 0; d < D; ++d) {
           const int j = jr[d];
           if (j >= 0 && !(NUMERIC && GRAM && j < row)) {
-            if (rt) insert_key_rt(keys, j, lg, a.status);
-            else insert_acc<LOG2T, NUMERIC>(keys, vals, j, NUMERIC ? __dmul_rn(ar[d], br[d]) : 0.0,
-                                            a.status);
+            insert_acc<LOG2T, NUMERIC>(keys, vals, j, NUMERIC ? __dmul_rn(ar[d], br[d]) : 0.0,
+                                       a.status);
           }
           if (NUMERIC) __syncwarp();  // k-order of the accumulation
         }
@@ -286,7 +260,7 @@ __global__ void __launch_bounds__(256, 5) k_hash_w32(RowArgs a) {
 
     if (!NUMERIC) {
       int c = 0, cl = 0;
-      for (int s = lane * 4; s < (1 << lg); s += 128) {
+      for (int s = lane * 4; s < T; s += 128) {
         const int4 k4 = *(const int4*)(keys + s);
         c += (k4.x != kEmptyKey) + (k4.y != kEmptyKey) + (k4.z != kEmptyKey) + (k4.w != kEmptyKey);
         if (GRAM)
