@@ -254,12 +254,32 @@ class Engine:
         return Plan(self, p, A, task)
 
     def multiply(self, A: CsrDevice, task: str = "AA", stream=None) -> CsrResult:
-        """C = A·A, A·Aᵀ ("AAt") or A·Aᵀ via the Gram path ("AAtS")."""
-        p = self.plan(A, task, stream)
+        """C = A·A, A·Aᵀ ("AAt") or A·Aᵀ via the Gram path ("AAtS").
+
+        The plan/execute pair of plan().execute() without the Plan object: one
+        stream lookup, only n and nnz(C) read from the plan's info, so that a
+        call on a small matrix spends little beyond the library's own time."""
+        sh = _stream_handle(stream)
+        s = A.struct()
+        L = lib()
+        p = ctypes.c_void_p()
+        check(L.spg_plan_create(self._h, _task_id(task), ctypes.byref(s), sh, ctypes.byref(p)),
+              "plan")
         try:
-            return p.execute(stream=stream)
+            info = SpgPlanInfo()
+            check(L.spg_plan_get_info(p, ctypes.byref(info)), "plan info")
+            n, nnz = int(info.n), int(info.nnz_c)
+            dev = A.rowptr.device
+            rp = torch.empty(n + 1, dtype=torch.int64, device=dev)
+            col = torch.empty(max(nnz, 1), dtype=torch.int32, device=dev)
+            val = torch.empty(max(nnz, 1), dtype=torch.float64, device=dev)
+            c = SpgCsrOut(n, 0, rp.data_ptr(), col.data_ptr(), val.data_ptr())
+            check(L.spg_execute(p, ctypes.byref(c), sh), "execute")
         finally:
-            p.close()
+            L.spg_plan_destroy(p)
+        if nnz != col.numel():
+            col, val = col[:nnz], val[:nnz]
+        return CsrResult(n, int(c.nnz), rp, col, val)
 
     def plan_batched(self, As, task: str = "AA", stream=None) -> Plan:
         """One plan for many independent products (block-diagonal layout)."""
