@@ -24,10 +24,6 @@ __device__ __forceinline__ unsigned lanemask_lt() {
   return m;
 }
 
-__device__ __forceinline__ int ld_volatile_shared(const int* p) {
-  return *(const volatile int*)p;
-}
-
 __device__ __forceinline__ void report(uint32_t* status, uint32_t bits) {
   atomicOr(status, bits);
 }
@@ -40,29 +36,7 @@ __device__ __forceinline__ unsigned hash_slot(int j) {
   return ((unsigned)j * 0x9E3779B1u) >> (32 - LOG2T);
 }
 
-// Open-addressing insert with linear probing into a shared table of 2^LOG2T
-// int keys.  A slot is read first (volatile, so every probe sees other lanes'
-// CAS results) and claimed with atomicCAS only when empty.  Returns the slot
-// of `j`, or −1 after 2^LOG2T probes (table full: reported, never spins).
-template <int LOG2T>
-__device__ __forceinline__ int hash_insert(int* keys, int j, uint32_t* status) {
-  constexpr unsigned T = 1u << LOG2T;
-  unsigned h = hash_slot<LOG2T>(j);
-#pragma unroll 1
-  for (unsigned probe = 0; probe < T; ++probe) {
-    int cur = ld_volatile_shared(keys + h);
-    if (cur == j) return (int)h;
-    if (cur == kEmptyKey) {
-      int old = atomicCAS(keys + h, kEmptyKey, j);
-      if (old == kEmptyKey || old == j) return (int)h;
-    }
-    h = (h + 1) & (T - 1);
-  }
-  report(status, DEV_ERR_HASH_FULL);
-  return -1;
-}
-
-// CAS-first linear probe of the warp kernels: one shared atomic per probe, the
+// CAS-first linear probe of the hash-table kernels: one shared atomic per probe, the
 // loop exits on an empty slot (claimed) or on the key itself (reading the slot
 // first and claiming only empty ones measured slower: 3.32 vs 2.88 ms for the
 // numeric phase of the 96³ stencil; so did claims without atomics — a round of

@@ -7,7 +7,8 @@
 // (row·n+col, value) pairs in hash order for a global radix sort.  Here:
 //  - the table is sized per bin and the group of lanes per row is sized with it
 //    (sub-warp groups for small tables, a whole CTA for the largest);
-//  - probes read first and CAS only empty slots;
+//  - each probe claims its slot with one CAS (claim-first), and a freshly
+//    claimed slot's value is set to 0.0 + a·b, so no value array is cleared;
 //  - the numeric phase walks row i of A in order and synchronises the group
 //    after each k, so every output value is Σ_k a_ik·b_kj added in increasing
 //    position of k with the product rounded first — the same sum the CPU
@@ -119,10 +120,7 @@ __device__ __forceinline__ void hash_row(const Grp& g, const RowArgs& a, const i
                                          int* st_bs, int* st_len, double* st_a, void* scratch,
                                          uint32_t* rtmp, int* rcnt) {
   constexpr int T = 1 << LOG2T;
-  for (int s = g.lane; s < T; s += g.G) {
-    keys[s] = kEmptyKey;
-    if (NUMERIC) vals[s] = 0.0;
-  }
+  for (int s = g.lane; s < T; s += g.G) keys[s] = kEmptyKey;
   const int32_t ps = a.A.rowptr[row], pe = a.A.rowptr[row + 1];
   for (int32_t pb = ps; pb < pe; pb += g.G) {
     const int cnt = min(g.G, pe - pb);
@@ -141,9 +139,10 @@ __device__ __forceinline__ void hash_row(const Grp& g, const RowArgs& a, const i
       for (int q = g.lane; q < len; q += g.G) {
         const int32_t j = a.B.col[bs + q];
         if (NUMERIC && GRAM && j < row) continue;
-        const int slot = hash_insert<LOG2T>(keys, j, a.status);
-        if (NUMERIC && slot >= 0)
-          vals[slot] = __dadd_rn(vals[slot], __dmul_rn(av, a.B.val[bs + q]));
+        // claim-first probe, as in the warp kernels (reading the slot before
+        // claiming measured slower: R-MAT 2^18 A·A 62.3 against 60.2 ms)
+        insert_acc<LOG2T, NUMERIC>(keys, vals, j,
+                                   NUMERIC ? __dmul_rn(av, a.B.val[bs + q]) : 0.0, a.status);
       }
       if (NUMERIC) g.sync();  // k-order of the accumulation
     }

@@ -178,7 +178,12 @@ __global__ void __launch_bounds__(256, 5) k_hash_w32(RowArgs a) {
         len = a.B.rowptr[k + 1] - bs;
         if (NUMERIC) av = a.A.val[pb + lane];
       }
-      constexpr int D = NUMERIC ? 4 : 8;
+      // B rows loaded ahead of the hashing: 3 (numeric) and 4 (symbolic) measured
+      // best on the 96³ stencil step and the 512-batch (numeric 2 / 4 / 6: 5.82 /
+      // 5.71 / 6.67 ms per step against 5.64; symbolic 2 / 3 / 8 / 16: 2.28 /
+      // 2.08 / 2.14 / 2.23 against 2.05): deeper staging costs registers and
+      // instructions in kernels that are issue-bound, not load-latency-bound
+      constexpr int D = NUMERIC ? 3 : 4;
       if (__all_sync(kFull, len <= 32)) {
         // Fast path: every B row of the chunk is one 32-wide segment.  Rows
         // t0..t0+D−1 are loaded together, then hashed in order.
