@@ -14,7 +14,7 @@
 //  - packs each occupied slot as ((col − lo) << log2T) | slot, sorts the
 //    packed words with a register bitonic network (E words per lane), and
 //    writes columns and the gathered values to the row's CSR slots; rows of
-//    more than 128 entries in tables of 512 slots and up sort the packed words
+//    more than 256 entries in tables of 512 slots and up sort the packed words
 //    with a stable LSD radix sort over the column bits instead, O(m) per
 //    digit rather than the bitonic network's O(m log² m), in the table's own
 //    free space.
@@ -30,9 +30,10 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 // Rows of more entries than this sort with the radix sort rather than the
-// register bitonic network (whose 8-per-lane form costs about 1,000 warp
-// instructions a row against about 600 for two or three digit passes).
-constexpr int kRadixMin = 128;
+// register bitonic network (8 words per lane up to 256 entries): measured on
+// the 512-matrix batch, a threshold of 256 against 128 gave 94.5–94.9 against
+// 95.5–96.7 ms, R-MAT 2^18 unchanged.
+constexpr int kRadixMin = 256;
 
 // Shared memory of one warp's row: the table's values (numeric) and keys.
 template <int LOG2T, bool NUMERIC>
