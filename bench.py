@@ -663,19 +663,29 @@ def serve_once(pool, ds, prods, rate, label, kw, picks, tasks, gaps):
             "peak_reserved_gb": round(st["peak_reserved_bytes"] / 1e9, 2)}
 
 
+def serve_stream(rate_index, stream, nreq, npool, rate):
+    """One arrival stream of the serving bench: matrix picks (indices into the
+    pool), tasks ("AA" / "AAt", 50/50) and exponential gaps at `rate` per
+    second, from numpy's PCG64 seeded with (55, rate_index, stream)."""
+    import numpy as np
+
+    rng = np.random.Generator(np.random.PCG64([55, rate_index, stream]))
+    picks = rng.integers(0, npool, nreq)
+    tasks = np.where(rng.random(nreq) < 0.5, "AA", "AAt")
+    gaps = rng.exponential(1.0 / rate, nreq)
+    return picks, tasks, gaps
+
+
 def serve_back_to_back(ds, prods, nreq):
     """The request mix as back-to-back plain calls: the first arrival stream's
     requests (matrix and task as the servers got them, no arrival gaps) through
     Engine.multiply one after another on one stream, each result freed before
     the next call; CUDA events around the whole sequence."""
-    import numpy as np
     import torch
 
     from appt_spgemm_b200.engine import Engine
 
-    rng = np.random.Generator(np.random.PCG64([55, 0, 0]))
-    picks = rng.integers(0, len(ds), nreq)
-    tasks = np.where(rng.random(nreq) < 0.5, "AA", "AAt")
+    picks, tasks, _ = serve_stream(0, 0, nreq, len(ds), 1.0)
     work = sum(2.0 * prods[(int(i), str(t))] for i, t in zip(picks, tasks))
     with Engine("cuda:0") as eng:
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -694,8 +704,6 @@ def serve_back_to_back(ds, prods, nreq):
 
 
 def run_serve(args):
-    import numpy as np
-
     from appt_spgemm_b200 import csr
     from appt_spgemm_b200.engine import CsrDevice
 
@@ -710,11 +718,8 @@ def run_serve(args):
     for ri, rate in enumerate(rates):
         for stream in range(args.serve_seeds):
             # one arrival stream per (rate, stream), run through both servers
-            rng = np.random.Generator(np.random.PCG64([55, ri, stream]))
             nreq = args.serve_requests
-            picks = rng.integers(0, len(pool), nreq)
-            tasks = np.where(rng.random(nreq) < 0.5, "AA", "AAt")
-            gaps = rng.exponential(1.0 / rate, nreq)
+            picks, tasks, gaps = serve_stream(ri, stream, nreq, len(pool), rate)
             for label, kw in SERVERS:
                 if label == "continuous_batching" and args.serve_workers > 0:
                     kw = dict(kw, workers=args.serve_workers)

@@ -196,3 +196,23 @@ def test_serve_pool_follows_its_recipe():
     first = bench.serve_pool(3, seed=5)
     assert [d for _, d in first] == [d for _, d in pool[:3]]
     assert all(a.nnz == b.nnz for (a, _), (b, _) in zip(first, pool))
+
+
+def test_serve_streams_are_seeded_per_rate_and_stream():
+    """Every arrival stream comes from (55, rate index, stream): the same
+    arguments give the same requests, the rate changes only the gaps (so the
+    back-to-back leg replays the first rate's first stream exactly), and the
+    tasks are A·A / A·Aᵀ with the gaps' mean near 1 / rate."""
+    import numpy as np
+
+    import bench
+    p1, t1, g1 = bench.serve_stream(0, 0, 2000, 40, 500.0)
+    p2, t2, g2 = bench.serve_stream(0, 0, 2000, 40, 1.0)
+    assert np.array_equal(p1, p2) and np.array_equal(t1, t2)
+    assert np.allclose(g2, g1 * 500.0)
+    assert set(np.unique(t1)) == {"AA", "AAt"} and 0.4 < np.mean(t1 == "AA") < 0.6
+    assert p1.min() >= 0 and p1.max() < 40
+    assert abs(np.mean(g1) * 500.0 - 1.0) < 0.1
+    p3, _, _ = bench.serve_stream(1, 0, 2000, 40, 500.0)
+    p4, _, _ = bench.serve_stream(0, 1, 2000, 40, 500.0)
+    assert not np.array_equal(p1, p3) and not np.array_equal(p1, p4)
